@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: plain FP64 F-cycle throughput of the multigrid engine on one B200 per rank.
+
+Workload (the reference's 513x257x129 case): u = x^3 y^2 z on [0,1]x[0,0.5]x[0,0.25],
+h = 1/512, 6 levels, BoundaryCondition {N,N,N,N,D,D} (resolved by the reference to Neumann
+on x, Dirichlet on y and z), FullWeighting + TrilinearInterpolation + weighted Jacobi
+(omega = 6/7), nsmooth = 2, F-cycles.  One step = one iteration of PoissonSolver::solve:
+one F-cycle, the fine residual with its max-norm, the norm read-back and the stopping rule.
+The metric is fine-grid DOF x F-cycles per second.
+
+  value  -- device-resident: K iterations of one solve() call, CUDA events on the engine's
+            stream, max over ranks; the 4 fine arrays (4 x 143 MB) are far larger than L2.
+  e2e    -- through the reference-facing API (mgp.PoissonSolver): per request
+            to_device (u, u_prev, f, r + faces from pinned host memory), a 4-cycle solve and
+            to_host (r, u, u_prev), timed on the same stream.
+  roofline -- the dominant kernel (the level-0 Jacobi sweep) timed alone with CUDA events,
+            against its algorithmic 24 B/point.
+  cpu_baseline -- the reference's own OpenMP build (oracle/_ref/ref_oracle) on this host.
+
+--impl reference runs the reference's CPU code instead (rank 0 only) with the same metric.
+Multi-GPU (torchrun): each rank solves its own independent replica (no collective on the
+data path): weak scaling, value = all ranks' DOF-cycles / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "multigrid-poisson_b200"))
+sys.path.insert(0, str(ROOT))
+
+DIMS = (513, 257, 129)
+LEVELS = 6
+H = 1.0 / 512
+BC = (1, 1, 1, 1, 0, 0)  # N S E W T B requested
+NSMOOTH = 2
+E2E_CYCLES = 4
+NDOF = DIMS[0] * DIMS[1] * DIMS[2]
+METRIC = "F-cycle fine-grid DOF/s (FP64, 513x257x129)"
+UNIT = "DOF*cycles/s"
+WORKLOAD = ("fp64 F-cycle, 513x257x129 (6 levels), u=x^3 y^2 z on [0,1]x[0,.5]x[0,.25], BC {N,N,N,N,D,D}, "
+            "FullWeighting + Trilinear + Jacobi(6/7), nsmooth=2; step = one solve() iteration")
+
+
+def problem2(x, y, z):
+    return x * x * x * y * y * z
+
+
+def rhs2(x, y, z):
+    return 2.0 * x * x * x * z + 6.0 * x * y * y * z
+
+
+def dudx2(x, y, z):
+    return 3.0 * x * x * y * y * z
+
+
+def dudy2(x, y, z):
+    return 2.0 * x * x * x * y * z
+
+
+def dudz2(x, y, z):
+    return x * x * x * y * y
+
+
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def __enter__(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.tmp,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.tmp is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.tmp.flush()
+        rows = []
+        for line in Path(self.tmp.name).read_text().splitlines():
+            t = [c.strip() for c in line.split(",")]
+            if len(t) >= 9:
+                rows.append(t)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows)}
+
+
+# ---------------------------------------------------------------------------------------
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x: float, local: int) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_solver(mgp, device: int, maxiter: int, pinned: bool):
+    st = mgp.Settings(levels=LEVELS, dims=list(DIMS), maxiter=maxiter, miniter=maxiter, tolerance=0.0,
+                      h=H, origin=[0.0, 0.0, 0.0], dev=device)
+    bc = mgp.BoundaryCondition(*BC)
+    ps = mgp.PoissonSolver(st, bc, restriction="FullWeighting", relaxation="Jacobi", dtype=mgp.F64,
+                           pinned=pinned)
+    ps.init(problem2, rhs2, dudx2, dudy2, dudz2)
+    return ps
+
+
+def kernel_roofline(mgp, ps, torch, stream, reps: int = 20):
+    """Average duration of the dominant kernel (level-0 Jacobi sweep), CUDA events on the
+    engine's stream; algorithmic bytes = 3 arrays x 8 B per shape point (read u_prev, read f,
+    write u)."""
+    eng = ps.engine
+    for _ in range(3):
+        eng.relax(0, -1.0, 1)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        eng.relax(0, -1.0, 1)
+    b.record(stream)
+    b.synchronize()
+    sec = a.elapsed_time(b) / 1e3 / reps
+    alg = 24.0 * NDOF
+    return sec, alg
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except (ValueError, KeyError):
+            pass
+    return 6650.0, "fallback"
+
+
+def cycle_model_bytes() -> float:
+    """Algorithmic bytes of one F-cycle + convergence check (FP64), composed from the
+    per-operation compulsory traffic: sweep 3sN, residual 3sN, FullWeighting s(N+Nc),
+    zero coarse u sNc, prolong+add s(2N+Nc), convergence check 2sN0."""
+    s = 8.0
+    dims = [tuple((d >> l) + 1 if l else d for d in DIMS) for l in range(LEVELS)]
+    n = [a * b * c for a, b, c in dims]
+    L = LEVELS
+    total = 0.0
+
+    def relax(l):
+        return NSMOOTH * 3 * s * n[l]
+
+    def setup(l):
+        return 3 * s * n[l] + s * (n[l] + n[l + 1]) + s * n[l + 1]
+
+    def padd(l):
+        return s * (2 * n[l] + n[l + 1])
+
+    def V(l):
+        t = relax(l)
+        if l >= L - 1:
+            return t
+        return t + setup(l) + V(l + 1) + padd(l) + relax(l)
+
+    def F(l):
+        t = relax(l) + setup(l)
+        if l < L - 2:
+            t += F(l + 1)
+        t += V(l + 1) + padd(l)
+        if l == 0:
+            t += V(0)
+        return t
+
+    total = F(0) + 2 * s * n[0]
+    return total
+
+
+def cpu_reference(steps: int, warm: int, threads: int | None = None):
+    """The reference's own OpenMP CPU build timed by its own solve_time()."""
+    from oracle.oracle import REF_BIN, RefRun
+
+    if not REF_BIN.exists():
+        return None
+    threads = threads or os.cpu_count() or 1
+    st = RefRun().run(DIMS, LEVELS, bc=BC, restriction="fw", relaxation="jacobi", problem=2, mode="time",
+                      cycle="Fcycle", nsmooth=NSMOOTH, maxiter=steps, tol=0.0, h=H, threads=threads,
+                      extra={"warm": warm, "timed": steps, "miniter": steps}, timeout=1800)
+    secs = st.stats["time"][-1]
+    iters = st.stats["iters"][-1]
+    return {"value": NDOF * iters / secs, "seconds": secs, "cycles": iters, "threads": threads}
+
+
+def run_reference_arm(args):
+    world, rank, local, pg = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    from oracle.oracle import REF_BIN
+
+    if not REF_BIN.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref/ref_oracle not built"}))
+        return 0
+    res = cpu_reference(args.steps, args.warmup)
+    cores = res["threads"]
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(1, res["cycles"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic x^3 y^2 z problem)", "config": {"workload": WORKLOAD},
+            "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{int(res['cycles'])} F-cycles on the full grid after {args.warmup} "
+                                       f"warm-up cycles, OMP_NUM_THREADS={cores}"},
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mgp", choices=["mgp", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    import torch
+
+    import mgp
+
+    torch.cuda.set_device(local)
+    # Each rank: an independent replica of the whole solve on its own GPU.
+    ps = build_solver(mgp, local, maxiter=args.steps, pinned=True)
+    ps.to_device()
+    eng = ps.engine
+    stream = torch.cuda.ExternalStream(eng.stream_handle, device=f"cuda:{local}")
+    # warm-up (captures and instantiates the CUDA graph)
+    eng.set_iteration_limits(args.warmup, args.warmup, 0.0)
+    eng.solve("Fcycle", NSMOOTH)
+    eng.set_iteration_limits(args.steps, args.steps, 0.0)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        st = eng.solve("Fcycle", NSMOOTH)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(pg)
+    sec = ev0.elapsed_time(ev1) / 1e3
+    assert st.cycles_run == args.steps, (st.cycles_run, args.steps)
+    tmax = max_over_ranks(pg, sec, local)
+    value = NDOF * args.steps * world / tmax
+
+    # e2e through the reference-facing API: to_device + solve(4 F-cycles) + to_host per request
+    eng.set_iteration_limits(E2E_CYCLES, E2E_CYCLES, 0.0)
+    ps.to_device()
+    ps.solve("Fcycle", NSMOOTH)
+    ps.to_host()
+    n_e2e = max(2, min(5, args.steps // 4))
+    barrier(pg)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_e2e):
+        ps.to_device()
+        ps.solve("Fcycle", NSMOOTH)
+        ps.to_host()
+    e1.record(stream)
+    e1.synchronize()
+    barrier(pg)
+    e2e_sec = max_over_ranks(pg, e0.elapsed_time(e1) / 1e3 / n_e2e, local)
+    e2e_value = NDOF * E2E_CYCLES * world / e2e_sec
+    esz = 8
+    lv = ps.engine.level[0]
+    face_elems = sum(a * b * c for a, b, c in lv.face_shape)
+    h2d = (4 * lv.size + face_elems) * esz
+    d2h = 3 * lv.size * esz
+
+    # dominant kernel roofline
+    ksec, kbytes = kernel_roofline(mgp, ps, torch, stream)
+    peak, peak_kind = measured_peaks()
+    achieved = kbytes / ksec / 1e9
+    cyc_bytes = cycle_model_bytes()
+    cyc_achieved = cyc_bytes / (sec / args.steps) / 1e9
+
+    if rank != 0:
+        return 0
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference(steps=2, warm=0)
+        except Exception as exc:  # noqa: BLE001 -- the baseline is informative only
+            cpu = {"error": str(exc)}
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tmax / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (analytic x^3 y^2 z problem on the host)",
+        "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (4 x 143 MB fine arrays)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "step": f"to_device + {E2E_CYCLES}-cycle solve + to_host", "ms_per_request": 1e3 * e2e_sec},
+        "roofline": {"bound": "hbm", "kernel": "k_stencil<double,OP_JACOBI> level 0", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "algorithmic_bytes_per_launch": kbytes, "launch_us": ksec * 1e6},
+        "cycle_roofline": {"model_bytes_per_cycle": cyc_bytes, "achieved": cyc_achieved, "peak": peak,
+                           "unit": "GB/s", "frac": cyc_achieved / peak, "ms_per_cycle": 1e3 * sec / args.steps},
+        "gpu_launches": int(st.kernel_launches),
+        "clocks": clocks,
+        "rel_res_after": st.rel_res,
+    }
+    if cpu and "value" in cpu:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["threads"], "kind": "reference",
+                                "sample": f"{int(cpu['cycles'])} F-cycles of the same workload, reference OpenMP "
+                                          f"build, OMP_NUM_THREADS={cpu['threads']}"}
+    elif cpu:
+        line["cpu_baseline"] = {"error": cpu.get("error")}
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,209 @@
+/*
+ * mgp.h -- C ABI of the B200-native geometric multigrid Poisson engine (libmgp.so).
+ *
+ * Plain C: pointers, sizes and status codes only.  This is the drop-in boundary under the
+ * reference's public solver API, Poisson::PoissonSolver<T,Restriction,Prolongation,Relaxation>
+ * of eljens/multigrid-poisson (include/libpoisson.h:28-67).  Each entry point names the
+ * reference interface it replaces.  The C++ header facade in
+ * multigrid-poisson_b200/poisson/libpoisson.h rebuilds that class on top of these calls.
+ *
+ * Conventions
+ *  - Every function returns an int status (mgp_status).  On failure a message is kept per
+ *    thread and returned by mgp_last_error().
+ *  - Host arrays exchanged with the engine use the reference's own halo-padded layout
+ *    (include/array.h:20-30,70-77):
+ *        idx(i,j,k) = (i+halo.west)*stride[0] + (j+halo.south)*stride[1] + (k+halo.bottom)
+ *        stride = {pad[1]*pad[2], pad[2], 1}, pad = shape + halo
+ *    mgp_level_info() returns shape, halo, pad, stride and size for every level.
+ *    Element type is double for MGP_F64 solvers and float for MGP_F32 solvers.
+ *  - Face (boundary-condition) arrays have no halo and the reference's face shapes
+ *    (include/domain.h:125-192): north/south (nx,1,nz), east/west (1,ny,nz),
+ *    top/bottom (nx,ny,1), k unit-stride.
+ *  - A solver owns all device memory of its level hierarchy, one CUDA stream and its cached
+ *    CUDA graphs.  A solver is not thread-safe; use one solver per host thread (the
+ *    reference's solver is not thread-safe either: GaussSeidel::alternate is mutable state).
+ */
+#ifndef MGP_H
+#define MGP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGP_ABI_VERSION 1
+
+/* Status codes.  The C++ facade maps INVALID_ARG to std::invalid_argument (reference:
+ * bad solver name include/libpoisson.h:242-244, bad dims src/domainsettings.cpp:20-27) and
+ * NO_DEVICE to std::runtime_error (include/devicearray.h:117-119). */
+typedef enum {
+    MGP_OK = 0,
+    MGP_ERR_INVALID_ARG = 1,
+    MGP_ERR_OOM = 2,
+    MGP_ERR_NO_DEVICE = 3,
+    MGP_ERR_CUDA = 4,
+    MGP_ERR_TIMEOUT = 5,
+    MGP_ERR_DIVERGED = 6,
+    MGP_ERR_UNSUPPORTED = 7,
+    MGP_ERR_STATE = 8
+} mgp_status;
+
+/* Boundary_t (include/boundary.h:14). */
+typedef enum { MGP_DIRICHLET = 0, MGP_NEUMANN = 1 } mgp_bc;
+/* Location_t order (include/boundary.h:12) -- also the field order of BoundaryCondition
+ * (include/boundary.h:23-30). */
+typedef enum { MGP_NORTH = 0, MGP_SOUTH = 1, MGP_EAST = 2, MGP_WEST = 3, MGP_TOP = 4, MGP_BOTTOM = 5 } mgp_face;
+/* Template plug-ins R, P, S of PoissonSolver<T,R,P,S>. */
+typedef enum { MGP_INJECTION = 0, MGP_FULLWEIGHTING = 1 } mgp_restriction;
+typedef enum { MGP_TRILINEAR = 0 } mgp_prolongation;
+typedef enum { MGP_JACOBI = 0, MGP_GAUSSSEIDEL = 1 } mgp_relaxation;
+/* T of PoissonSolver<T,...>. */
+typedef enum { MGP_F64 = 0, MGP_F32 = 1 } mgp_dtype;
+/* DeviceArray members of Domain<T> (include/domain.h:62-65). */
+typedef enum { MGP_FIELD_U = 0, MGP_FIELD_UPREV = 1, MGP_FIELD_F = 2, MGP_FIELD_R = 3 } mgp_field;
+/* solve("relaxation"|"Vcycle"|"Fcycle") (include/libpoisson.h:239-244). */
+typedef enum { MGP_CYCLE_RELAXATION = 0, MGP_CYCLE_V = 1, MGP_CYCLE_F = 2 } mgp_cycle;
+
+/* mgp_desc.flags */
+#define MGP_FLAG_STRICT_BC 1u /* honour the requested north/south/bottom kinds instead of the
+                                 reference's resolution to Dirichlet (include/domain.h:140-145,191-192) */
+
+/* Settings (include/settings.h:14-39) plus the BoundaryCondition and the template choice. */
+typedef struct mgp_desc {
+    int64_t dims[3];   /* Settings::dims */
+    int64_t levels;    /* Settings::levels */
+    int64_t maxiter;   /* Settings::maxiter */
+    int64_t miniter;   /* Settings::miniter (reference default 1) */
+    double tolerance;  /* Settings::tolerance */
+    double h;          /* Settings::h, uniform spacing */
+    double origin[3];  /* Settings::origin */
+    int32_t bc[6];     /* requested mgp_bc per face, mgp_face order */
+    int32_t restriction;
+    int32_t prolongation;
+    int32_t relaxation;
+    int32_t dtype;
+    int32_t device;    /* CUDA device ordinal */
+    uint32_t flags;
+} mgp_desc;
+
+/* Geometry of one level: DomainSettings(l) (src/domainsettings.cpp:12-29) and the
+ * host array layout of Domain<T>'s arrays (include/domain.h:102-121). */
+typedef struct mgp_level_info {
+    int64_t shape[3];
+    int64_t halo[6]; /* east, west, north, south, top, bottom (Halo, include/halo.h:6-34) */
+    int64_t pad[3];
+    int64_t stride[3];
+    int64_t size;    /* elements of one host field array */
+    double h;
+    double origin[3];
+    int32_t face_kind[6];      /* resolved mgp_bc per face, mgp_face order */
+    int64_t face_shape[6][3];
+} mgp_level_info;
+
+/* Results of PoissonSolver::solve: relative_residual(), solve_iterations(), solve_time()
+ * (include/libpoisson.h:377-393). */
+typedef struct mgp_stats {
+    double rel_res;
+    double iterations;  /* loop index at exit, as the reference reports it */
+    double seconds;
+    int64_t cycles_run; /* cycles actually executed */
+    double first_rel_res;   /* relative residual before the first cycle */
+    int64_t kernel_launches; /* CUDA kernels this call launched (graph nodes included) */
+} mgp_stats;
+
+/* mgp_solve flags */
+#define MGP_SOLVE_VERBOSE 1u          /* PoissonSolver::verbose(true) prints (:286-288, :337-339) */
+#define MGP_SOLVE_PRINT_CYCLE_TIME 2u /* the reference's unconditional "Vcycle took ..." line (:297,:302) */
+
+typedef struct mgp_solver mgp_solver;
+
+const char* mgp_status_string(int status);
+/* Last error message of the calling thread ("" if none). */
+const char* mgp_last_error(void);
+int mgp_abi_version(void);
+/* Number of visible CUDA devices (omp_get_num_devices() in the reference drivers). */
+int mgp_device_count(int* n);
+
+/* PoissonSolver(Settings&, BoundaryCondition&) (include/libpoisson.h:80-87) with
+ * PoissonSolver::alloc (:112-156): builds the level hierarchy (Grid, src/grid.cpp:6-13)
+ * and allocates every level's arrays on the device, zero-initialised.
+ * Errors: INVALID_ARG for non-coarsenable dims (src/domainsettings.cpp:20-27) or a bad
+ * descriptor; UNSUPPORTED for red-black Gauss-Seidel on a layout whose padded z extent is
+ * even (the reference's colouring degenerates and its result depends on thread timing);
+ * NO_DEVICE; OOM. */
+int mgp_create(const mgp_desc* desc, mgp_solver** out);
+/* ~PoissonSolver (include/libpoisson.h:100-110). */
+int mgp_destroy(mgp_solver* s);
+int mgp_level_info_get(const mgp_solver* s, int level, mgp_level_info* out);
+/* The same geometry from a descriptor alone, without a device: validates `desc` exactly as
+ * mgp_create does (INVALID_ARG for bad dims/levels/kinds, UNSUPPORTED for a degenerate
+ * red-black colouring) and fills the host layout of `level` (DomainSettings(l) and the
+ * Domain<T> halo widths and face kinds, include/domain.h:100-193). */
+int mgp_plan_level(const mgp_desc* desc, int level, mgp_level_info* out);
+int mgp_num_levels(const mgp_solver* s);
+
+/* DeviceArray<T>::to_device / to_host (include/devicearray.h:71-110) of one field of one
+ * level.  host points to `count` elements in the reference layout of that level
+ * (count must equal mgp_level_info.size).  Only shape points are transferred; the halo
+ * entries of a host array are left untouched by downloads and ignored by uploads. */
+int mgp_upload_field(mgp_solver* s, int field, int level, const void* host, int64_t count);
+int mgp_download_field(mgp_solver* s, int field, int level, void* host, int64_t count);
+/* Boundary<T>::arr to_device (dirichlet.h:232-235, neumann.h:511-514) and back. */
+int mgp_upload_face(mgp_solver* s, int face, int level, const void* host, int64_t count);
+int mgp_download_face(mgp_solver* s, int face, int level, void* host, int64_t count);
+/* Domain<T>::write_bc_to(u) and (u_prev) as done at the end of Domain::to_device
+ * (include/domain.h:259-262, 318-326): Dirichlet face data into the boundary planes, in
+ * the reference's face order so that later faces win on shared edges. */
+int mgp_write_bc(mgp_solver* s, int level);
+
+/* PoissonSolver::solve (include/libpoisson.h:237-357) on the device: initial norms, the
+ * cycle loop (each iteration one CUDA-graph launch holding the whole cycle plus the fine
+ * residual and its max-norm) and the reference's stopping rule.  omega < 0 selects the
+ * relaxation's default (6/7 Jacobi, 8/9 Gauss-Seidel).  ofile may be NULL or "" (no log).
+ * INVALID_ARG for an F-cycle with fewer than 2 levels (the reference indexes past its
+ * hierarchy there). */
+int mgp_solve(mgp_solver* s, int cycle, int64_t nsmooth, double omega, const char* ofile, double maxtime,
+              uint32_t flags, mgp_stats* out);
+/* Settings::maxiter / miniter / tolerance after construction. */
+int mgp_set_iteration_limits(mgp_solver* s, int64_t maxiter, int64_t miniter, double tolerance);
+
+/* ---- operator entry points (the reference's operator plug-ins, one level each) ---- */
+/* Relaxation<T>::relax (include/relaxation.h:19-94): smoothing_multiplier()*nsmooth
+ * half-sweeps (Jacobi ping-pong / red-black SOR) with the Neumann ghost values formed in
+ * the kernel. */
+int mgp_relax(mgp_solver* s, int level, double omega, int64_t nsmooth);
+/* residual<T>(Domain&) (include/residual.h:17-81). */
+int mgp_residual(mgp_solver* s, int level);
+/* Restriction<T>::restrict_to(r_l, f_{l+1}) (injection.h:29-67 / fullweighting.h:37-122). */
+int mgp_restrict(mgp_solver* s, int level);
+/* DeviceArray<T>::init_zero of u_{l} (include/devicearray.h:132-159). */
+int mgp_zero_u(mgp_solver* s, int level);
+/* The six Boundary<T>::restrict_to calls from level l to l+1 (include/vcycle.h:52-75). */
+int mgp_restrict_bc(mgp_solver* s, int level);
+/* TrilinearInterpolation::prolong(u_{l+1}, r_l) (include/trilinearinterpolation.h:29-134). */
+int mgp_prolong(mgp_solver* s, int level);
+/* DeviceArray<T>::add(r_l) into u_l (include/devicearray.h:161-196). */
+int mgp_add(mgp_solver* s, int level);
+/* prolong followed by add, fused: u_l += P u_{l+1} without materialising P u_{l+1}
+ * in r_l's interior (the form the cycles use). */
+int mgp_prolong_add(mgp_solver* s, int level);
+/* Vcycle<T> / Fcycle<T> from `level` (include/vcycle.h:14-98, include/fcycle.h:13-97). */
+int mgp_vcycle(mgp_solver* s, int level, double omega, int64_t nsmooth);
+int mgp_fcycle(mgp_solver* s, int level, double omega, int64_t nsmooth);
+/* DeviceArray<T>::infinity_norm (include/devicearray.h:198-240), returned as double. */
+int mgp_norm(mgp_solver* s, int field, int level, double* out);
+/* Waits for all work queued on the solver's stream. */
+int mgp_synchronize(mgp_solver* s);
+/* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
+int mgp_get_stream(mgp_solver* s, void** stream);
+
+/* Page-locked host memory for field buffers (faster uploads/downloads). */
+int mgp_host_alloc(void** p, size_t bytes);
+int mgp_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGP_H */

@@ -1,0 +1,370 @@
+// mgp_kernels.cuh -- sm_100a stencil kernels of the multigrid engine.
+//
+// Device layout (one per level, shared by u, u_prev, f and r): shape points only, no ghost
+// cells, k (z) unit-stride, rows padded to a 64-byte pitch:
+//     off(i,j,k) = i*sx + j*sy + k,   sy = round_up(nz, 64/sizeof(T)),  sx = sy*ny.
+// Neumann ghost values are never stored: each kernel forms them where it needs them, with
+// the reference's arithmetic  ghost = (sign*2h)*g + u[mirror]  (include/neumann.h:63-131),
+// which is exactly what the reference writes into its ghost layer before every sweep.
+//
+// Arithmetic follows the reference's expressions operand for operand, including its
+// promotions for T=float (double literals such as 6.0 and 0.5 promote a float expression
+// to double).  The library is compiled with --fmad=false, so no multiply-add is contracted
+// and FP64 results match the CPU reference bit for bit.
+//
+// Stencil kernels use a 2.5-D march: one thread per (j,k) column of a plane, marching i
+// over a chunk of planes with u(i-1), u(i), u(i+1) in registers; in-plane neighbours come
+// through the read-only data path (L1).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mgp {
+
+enum Face { F_NORTH = 0, F_SOUTH = 1, F_EAST = 2, F_WEST = 3, F_TOP = 4, F_BOTTOM = 5 };
+
+struct Geom {
+    int nx, ny, nz;
+    long long sx, sy;
+    int x0, x1, y0, y1, z0, z1;  // relaxation/residual bounds (is_non_eliminated, relaxation.h:78-83)
+    int poff;                    // red-black colour offset
+};
+
+template <typename T>
+struct Faces {
+    const T* g[6];  // dense face arrays, reference face layout
+};
+
+template <typename T>
+__device__ __forceinline__ T ldg(const T* p) {
+    return __ldg(p);
+}
+
+// Non-negative floating values order like their bit patterns; NaN (sign cleared) sorts
+// above +inf, so a NaN residual propagates into the norm.
+__device__ __forceinline__ unsigned long long abs_bits(double v) {
+    return (unsigned long long)__double_as_longlong(fabs(v));
+}
+__device__ __forceinline__ unsigned long long abs_bits(float v) {
+    return (unsigned long long)__double_as_longlong(fabs((double)v));
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+// Block-wide max, then one atomicMax per block.
+__device__ __forceinline__ void block_max_to(unsigned long long v, unsigned long long* out) {
+    __shared__ unsigned long long red[32];
+    v = warp_max_u64(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        unsigned long long w = lane < nw ? red[lane] : 0ull;
+        w = warp_max_u64(w);
+        if (lane == 0 && w) atomicMax(out, w);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Stencil ops.
+enum StencilOp { OP_JACOBI = 0, OP_GS = 1, OP_GS_COLUMN = 2, OP_RESIDUAL = 3 };
+
+template <typename T>
+struct StencilArgs {
+    Geom G;
+    const T* src;  // u (or u_prev for Jacobi)
+    T* dst;        // u for Jacobi/GS, r for the residual
+    const T* f;
+    Faces<T> F;
+    T two_h;       // 2*h of this level (T, as the reference's two_h)
+    T hsq;         // h*h (T)
+    T one_omega;   // 1-omega (T)
+    T omega_sixth; // omega/6 (T)
+    int colour;    // GS colour (0 red: idx%2==0, 1 black)
+    int ichunk;    // planes per block
+    unsigned long long* norm;  // residual: max |r| over the whole shape (nullptr: none)
+};
+
+// Residual with the reference's promotions: f - (sum - 6.0*u)/hsq (include/residual.h:70-72).
+__device__ __forceinline__ double residual_expr(double f, double sum, double u, double hsq) {
+    return f - (sum - 6.0 * u) / hsq;
+}
+__device__ __forceinline__ float residual_expr(float f, float sum, float u, float hsq) {
+    return (float)((double)f - ((double)sum - 6.0 * (double)u) / (double)hsq);
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
+    const Geom& G = a.G;
+    const int plane = G.ny * G.nz;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ia = blockIdx.y * a.ichunk;
+    const int ib = min(G.nx, ia + a.ichunk);
+    unsigned long long mx = 0ull;
+    if (t < plane) {
+        const int j = t / G.nz;
+        const int k = t - j * G.nz;
+        const long long bjk = (long long)j * G.sy + k;
+        const bool in_jk = (j >= G.y0) && (j < G.y1) && (k >= G.z0) && (k < G.z1);
+        int i0 = max(ia, G.x0), i1 = min(ib, G.x1);
+        if (!in_jk) i1 = i0;  // no stencil work in this column
+        if (OP == OP_RESIDUAL && a.norm) {
+            // r outside the bounds keeps its value and still counts in the norm
+            // (infinity_norm runs over the whole shape, devicearray.h:221-237).
+            for (int i = ia; i < ib; i++) {
+                if (i >= i0 && i < i1) continue;
+                mx = max(mx, abs_bits(a.dst[(long long)i * G.sx + bjk]));
+            }
+        }
+        if (i0 < i1) {
+            // src may alias dst (in-place Gauss-Seidel): reads go through ldg() and only touch
+            // points of the colour this pass does not write.
+            const T* src = a.src;
+            const T* f = a.f;
+            const T two_h = a.two_h;
+            // u(i0-1): a stored value or the west ghost  -2h*gW + u(1)
+            T vc = ldg(src + (long long)i0 * G.sx + bjk);
+            T vm;
+            if (i0 > 0) vm = ldg(src + (long long)(i0 - 1) * G.sx + bjk);
+            else vm = (-two_h) * ldg(a.F.g[F_WEST] + (long long)j * G.nz + k) + ldg(src + G.sx + bjk);
+            T vm_old = vm;  // u(i-1) before this sweep touched it (mirror of the east ghost)
+            for (int i = i0; i < i1; i++) {
+                const long long p = (long long)i * G.sx + bjk;
+                T vp;
+                if (i + 1 < G.nx) vp = ldg(src + p + G.sx);
+                else vp = two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + k) + vm_old;
+                bool active = true;
+                if (OP == OP_GS) active = ((i + j + k + G.poff) & 1) == a.colour;
+                if (OP == OP_GS_COLUMN) active = ((j + k + G.poff) & 1) == a.colour;
+                T vc_old = vc;
+                if (active) {
+                    T ym, yp, zm, zp;
+                    if (j > 0) ym = ldg(src + p - G.sy);
+                    else ym = (-two_h) * ldg(a.F.g[F_SOUTH] + (long long)i * G.nz + k) + ldg(src + p + G.sy);
+                    if (j < G.ny - 1) yp = ldg(src + p + G.sy);
+                    else yp = two_h * ldg(a.F.g[F_NORTH] + (long long)i * G.nz + k) + ldg(src + p - G.sy);
+                    if (k > 0) zm = ldg(src + p - 1);
+                    else zm = (-two_h) * ldg(a.F.g[F_BOTTOM] + (long long)i * G.ny + j) + ldg(src + p + 1);
+                    if (k < G.nz - 1) zp = ldg(src + p + 1);
+                    else zp = two_h * ldg(a.F.g[F_TOP] + (long long)i * G.ny + j) + ldg(src + p - 1);
+                    const T sum = vm + vp + ym + yp + zm + zp;
+                    if (OP == OP_RESIDUAL) {
+                        const T r = residual_expr(ldg(f + p), sum, vc, a.hsq);
+                        a.dst[p] = r;
+                        mx = max(mx, abs_bits(r));
+                    } else {
+                        // jacobi.h:59-61 / gaussseidel.h:43-45:
+                        //   u = one_omega*v + omega_sixth*(sum - hsq*f)
+                        const T nv = a.one_omega * vc + a.omega_sixth * (sum - a.hsq * ldg(f + p));
+                        a.dst[p] = nv;
+                        vc = nv;
+                    }
+                }
+                vm_old = vc_old;
+                vm = vc;
+                vc = vp;
+            }
+        }
+    }
+    if (OP == OP_RESIDUAL && a.norm) block_max_to(mx, a.norm);
+}
+
+// ------------------------------------------------------------------------------------
+// Restriction r_l -> f_{l+1} over the coarse shape, with u_{l+1} = 0 fused in
+// (include/vcycle.h:43-50).  Works on any pair of (shape, strides) views, so the same code
+// restricts the 2-D face arrays of Neumann::restrict_to.
+struct View {
+    int n[3];
+    long long s0, s1;  // k unit-stride
+};
+
+template <typename T>
+__device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j, int k) {
+    // FullWeighting::restrict_to (include/fullweighting.h:66-109): weights (1,2,1)^3/64 with
+    // indices clamped to the array; sums in the reference's order, double accumulators.
+    const int ii = min(vi.n[0] - 1, 2 * i), jj = min(vi.n[1] - 1, 2 * j), kk = min(vi.n[2] - 1, 2 * k);
+    const int im = max(0, ii - 1), ip = min(vi.n[0] - 1, ii + 1);
+    const int jm = max(0, jj - 1), jp = min(vi.n[1] - 1, jj + 1);
+    const int km = max(0, kk - 1), kp = min(vi.n[2] - 1, kk + 1);
+    auto A = [&](int x, int y, int z) -> double { return (double)ldg(in + x * vi.s0 + y * vi.s1 + z); };
+    const double s_m = 1.0 * A(im, jm, km) + 2.0 * A(im, jj, km) + 1.0 * A(im, jp, km) + 2.0 * A(ii, jm, km) +
+                       4.0 * A(ii, jj, km) + 2.0 * A(ii, jp, km) + 1.0 * A(ip, jm, km) + 2.0 * A(ip, jj, km) +
+                       1.0 * A(ip, jp, km);
+    T tmp = (T)s_m;
+    const double s_0 = 2.0 * A(im, jm, kk) + 4.0 * A(im, jj, kk) + 2.0 * A(im, jp, kk) + 4.0 * A(ii, jm, kk) +
+                       8.0 * A(ii, jj, kk) + 4.0 * A(ii, jp, kk) + 2.0 * A(ip, jm, kk) + 4.0 * A(ip, jj, kk) +
+                       2.0 * A(ip, jp, kk);
+    tmp = (T)((double)tmp + s_0);
+    const double s_p = 1.0 * A(im, jm, kp) + 2.0 * A(im, jj, kp) + 1.0 * A(im, jp, kp) + 2.0 * A(ii, jm, kp) +
+                       4.0 * A(ii, jj, kp) + 2.0 * A(ii, jp, kp) + 1.0 * A(ip, jm, kp) + 2.0 * A(ip, jj, kp) +
+                       1.0 * A(ip, jp, kp);
+    tmp = (T)((double)tmp + s_p);
+    return (T)((double)tmp / 64.0);
+}
+
+template <typename T, bool FW>
+__global__ void __launch_bounds__(256) k_restrict(const T* __restrict__ in, View vi, T* __restrict__ out, View vo,
+                                                  T* __restrict__ zero_u) {
+    const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % vo.n[2]);
+        const long long q = t / vo.n[2];
+        const int j = (int)(q % vo.n[1]);
+        const int i = (int)(q / vo.n[1]);
+        const long long o = i * vo.s0 + j * vo.s1 + k;
+        T v;
+        if (FW) v = fw_point(in, vi, i, j, k);
+        else v = ldg(in + (2 * i) * vi.s0 + (2 * j) * vi.s1 + 2 * k);  // injection.h:63
+        out[o] = v;
+        if (zero_u) zero_u[o] = T(0);
+    }
+}
+
+// Neumann::restrict_to (include/neumann.h:146-252) for every Neumann face of the coarse
+// level: g_c = R(g_f) - (c1*u0 + c2*u1 + c3*u2)/h_f.  blockIdx.y selects the face.
+template <typename T>
+struct BcRestrictArgs {
+    const T* gf[6];
+    T* gc[6];
+    View vf[6], vc[6];
+    int neumann[6];
+    const T* u;  // fine u
+    Geom Gf;     // fine level geometry (strides of u)
+    T h;         // fine h
+    bool fw;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
+    const int fc = blockIdx.y;
+    if (!a.neumann[fc]) return;
+    const View vo = a.vc[fc];
+    const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
+    const int nxf = a.Gf.nx, nyf = a.Gf.ny, nzf = a.Gf.nz;
+    int offx = 0, offy = 0, offz = 0, ii = 0, jj = 0, kk = 0, iii = 0, jjj = 0, kkk = 0;
+    T c1 = T(-3.0 / 2.0), c2 = T(2.0), c3 = T(-0.5);
+    switch (fc) {
+        case F_EAST: offx = nxf / 2; ii = -1; iii = -2; break;
+        case F_WEST: ii = 1; iii = 2; break;
+        case F_NORTH: offy = nyf / 2; jj = -1; jjj = -2; break;
+        case F_SOUTH: jj = 1; jjj = 2; break;
+        case F_TOP: offz = nzf / 2; kk = -1; kkk = -2; break;
+        default: kk = 1; kkk = 2; break;
+    }
+    if (fc == F_EAST || fc == F_NORTH || fc == F_TOP) {
+        c3 = T(0.5);
+        c2 = T(-2.0);
+        c1 = T(3.0 / 2.0);
+    }
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % vo.n[2]);
+        const long long q = t / vo.n[2];
+        const int j = (int)(q % vo.n[1]);
+        const int i = (int)(q / vo.n[1]);
+        T g = a.fw ? fw_point(a.gf[fc], a.vf[fc], i, j, k)
+                   : ldg(a.gf[fc] + (2 * i) * a.vf[fc].s0 + (2 * j) * a.vf[fc].s1 + 2 * k);
+        const int x = 2 * (i + offx), y = 2 * (j + offy), z = 2 * (k + offz);
+        auto U = [&](int xx, int yy, int zz) -> T { return ldg(a.u + xx * a.Gf.sx + yy * a.Gf.sy + zz); };
+        g -= (c1 * U(x, y, z) + c2 * U(x + ii, y + jj, z + kk) + c3 * U(x + iii, y + jjj, z + kkk)) / a.h;
+        a.gc[fc][i * vo.s0 + j * vo.s1 + k] = g;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Trilinear prolongation (include/trilinearinterpolation.h:29-134), evaluated per fine
+// point with the reference's pass structure: inject even points, then x, y and z midpoints
+// of the previous passes' values.  ADD: u += P e (DeviceArray::add, devicearray.h:161-196);
+// r receives P e on points outside the relaxation bounds (where the reference's r keeps it
+// until the next prolongation) or, when !ADD, everywhere.
+template <typename T>
+__device__ __forceinline__ T half_sum(T a, T b) {
+    return (T)(0.5 * (a + b));
+}
+
+template <typename T, bool ADD>
+__global__ void __launch_bounds__(256) k_prolong(const T* __restrict__ uc, Geom Gc, T* u, T* r, Geom Gf) {
+    const long long n = (long long)Gf.nx * Gf.ny * Gf.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % Gf.nz);
+        const long long q = t / Gf.nz;
+        const int j = (int)(q % Gf.ny);
+        const int i = (int)(q / Gf.ny);
+        const int ic = i >> 1, jc = j >> 1, kc = k >> 1;
+        auto C = [&](int x, int y, int z) -> T { return ldg(uc + x * Gc.sx + y * Gc.sy + z); };
+        auto X = [&](int y, int z) -> T {  // value at (i, 2y, 2z) after the x pass
+            T v = C(ic, y, z);
+            if (i & 1) v = half_sum(v, C(ic + 1, y, z));
+            return v;
+        };
+        auto Y = [&](int z) -> T {  // value at (i, j, 2z) after the y pass
+            if (j & 1) return half_sum(X(jc, z), X(jc + 1, z));
+            return X(jc, z);
+        };
+        const T e = (k & 1) ? half_sum(Y(kc), Y(kc + 1)) : Y(kc);
+        const long long p = (long long)i * Gf.sx + (long long)j * Gf.sy + k;
+        if (ADD) {
+            u[p] = u[p] + e;
+            const bool inside = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1 && k >= Gf.z0 && k < Gf.z1;
+            if (!inside) r[p] = e;
+        } else {
+            r[p] = e;
+        }
+    }
+}
+
+// u += r over the shape (DeviceArray::add).
+template <typename T>
+__global__ void __launch_bounds__(256) k_add(T* u, const T* __restrict__ r, Geom G) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
+        u[p] = u[p] + ldg(r + p);
+    }
+}
+
+// max |a| over the shape (DeviceArray::infinity_norm).
+template <typename T>
+__global__ void __launch_bounds__(256) k_norm(const T* __restrict__ a, Geom G, unsigned long long* out) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    unsigned long long mx = 0ull;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        mx = max(mx, abs_bits(ldg(a + (long long)i * G.sx + (long long)j * G.sy + k)));
+    }
+    block_max_to(mx, out);
+}
+
+// Dirichlet::write_to (include/dirichlet.h:50-93): one face into its boundary plane.
+template <typename T>
+__global__ void __launch_bounds__(256) k_write_face(T* u, Geom G, const T* __restrict__ g, int fc) {
+    int n0, n1;  // face extents in its two free dimensions
+    if (fc == F_EAST || fc == F_WEST) { n0 = G.ny; n1 = G.nz; }
+    else if (fc == F_NORTH || fc == F_SOUTH) { n0 = G.nx; n1 = G.nz; }
+    else { n0 = G.nx; n1 = G.ny; }
+    const long long n = (long long)n0 * n1;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t % n1), a0 = (int)(t / n1);
+        int i, j, k;
+        if (fc == F_EAST || fc == F_WEST) { i = fc == F_EAST ? G.nx - 1 : 0; j = a0; k = b; }
+        else if (fc == F_NORTH || fc == F_SOUTH) { i = a0; j = fc == F_NORTH ? G.ny - 1 : 0; k = b; }
+        else { i = a0; j = b; k = fc == F_TOP ? G.nz - 1 : 0; }
+        u[(long long)i * G.sx + (long long)j * G.sy + k] = g[t];
+    }
+}
+
+}  // namespace mgp
