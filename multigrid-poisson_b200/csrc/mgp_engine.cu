@@ -165,12 +165,14 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     a.omega_sixth = (T)(omega / 6.0);
     a.colour = colour;
     a.norm = norm;
-    const int plane = L.G.ny * L.G.nz;
+    constexpr int V = VecT<T>::V;
+    const int plane = L.G.ny * ((L.G.nz + V - 1) / V);  // threads per plane
     const int bx = (plane + kThreads - 1) / kThreads;
     int chunks = 1;
     if (OP != OP_GS_COLUMN) {
+        // enough blocks for ~2 waves; small levels get one plane per thread
         const int target = sm_count(s->device) * 8;
-        chunks = std::max(1, std::min((target + bx - 1) / bx, std::max(1, L.G.nx / 8)));
+        chunks = std::max(1, std::min((target + bx - 1) / bx, L.G.nx));
     }
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
@@ -265,9 +267,10 @@ template <typename T, bool ADD>
 int prolong_t(mgp_solver* s, int l) {
     LevelState& F = s->lv[l];
     LevelState& C = s->lv[l + 1];
-    const long long n = (long long)F.G.nx * F.G.ny * F.G.nz;
-    k_prolong<T, ADD><<<grid_1d(s, n), kThreads, 0, s->stream>>>((const T*)u_ptr(s, l + 1), C.G, (T*)u_ptr(s, l),
-                                                                   (T*)F.r, F.G);
+    constexpr int V = VecT<T>::V;
+    const int rows = F.G.ny * ((F.G.nz + V - 1) / V);
+    dim3 grid((rows + kThreads - 1) / kThreads, F.G.nx);
+    k_prolong<T, ADD><<<grid, kThreads, 0, s->stream>>>((const T*)u_ptr(s, l + 1), C.G, (T*)u_ptr(s, l), (T*)F.r, F.G);
     return check_launch(s);
 }
 

@@ -101,76 +101,204 @@ __device__ __forceinline__ float residual_expr(float f, float sum, float u, floa
     return (float)((double)f - ((double)sum - 6.0 * (double)u) / (double)hsq);
 }
 
+// 16-byte vectors along k: 2 doubles or 4 floats per thread.  Rows are 64-byte aligned, so
+// a vector starting at a multiple of V is aligned.
+template <typename T>
+struct VecT;
+template <>
+struct VecT<double> {
+    static constexpr int V = 2;
+    using type = double2;
+};
+template <>
+struct VecT<float> {
+    static constexpr int V = 4;
+    using type = float4;
+};
+
+__device__ __forceinline__ void ldv(double (&d)[2], const double* p) {
+    const double2 x = __ldg(reinterpret_cast<const double2*>(p));
+    d[0] = x.x;
+    d[1] = x.y;
+}
+__device__ __forceinline__ void ldv(float (&d)[4], const float* p) {
+    const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+    d[0] = x.x;
+    d[1] = x.y;
+    d[2] = x.z;
+    d[3] = x.w;
+}
+// plain (coherent) vector loads for arrays the same kernel writes
+__device__ __forceinline__ void ldv_rw(double (&d)[2], const double* p) {
+    const double2 x = *reinterpret_cast<const double2*>(p);
+    d[0] = x.x;
+    d[1] = x.y;
+}
+__device__ __forceinline__ void ldv_rw(float (&d)[4], const float* p) {
+    const float4 x = *reinterpret_cast<const float4*>(p);
+    d[0] = x.x;
+    d[1] = x.y;
+    d[2] = x.z;
+    d[3] = x.w;
+}
+__device__ __forceinline__ void stv(double* p, const double (&d)[2]) {
+    *reinterpret_cast<double2*>(p) = make_double2(d[0], d[1]);
+}
+__device__ __forceinline__ void stv(float* p, const float (&d)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(d[0], d[1], d[2], d[3]);
+}
+
+// One thread owns a V-vector of k points of one (j) row and marches i over a chunk of
+// planes; the next plane of u and f are prefetched one step ahead.  For small levels the
+// chunk is a single plane, which turns the march into one point-vector per thread.
 template <typename T, int OP>
 __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
+    constexpr int V = VecT<T>::V;
     const Geom& G = a.G;
-    const int plane = G.ny * G.nz;
+    const int nv = (G.nz + V - 1) / V;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int ia = blockIdx.y * a.ichunk;
     const int ib = min(G.nx, ia + a.ichunk);
     unsigned long long mx = 0ull;
-    if (t < plane) {
-        const int j = t / G.nz;
-        const int k = t - j * G.nz;
-        const long long bjk = (long long)j * G.sy + k;
-        const bool in_jk = (j >= G.y0) && (j < G.y1) && (k >= G.z0) && (k < G.z1);
-        int i0 = max(ia, G.x0), i1 = min(ib, G.x1);
-        if (!in_jk) i1 = i0;  // no stencil work in this column
+    if (t < G.ny * nv) {
+        const int j = t / nv;
+        const int kb = (t - j * nv) * V;
+        const long long bjk = (long long)j * G.sy + kb;
+        const bool jin = j >= G.y0 && j < G.y1;
+        unsigned ins = 0u, inr = 0u;  // elements inside the shape / inside the relaxation bounds
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const int k = kb + e;
+            if (k < G.nz) ins |= 1u << e;
+            if (jin && k >= G.z0 && k < G.z1) inr |= 1u << e;
+        }
+        const unsigned full = (1u << V) - 1u;
+        const int i0 = max(ia, G.x0);
+        const int i1 = inr ? min(ib, G.x1) : i0;
         if (OP == OP_RESIDUAL && a.norm) {
             // r outside the bounds keeps its value and still counts in the norm
             // (infinity_norm runs over the whole shape, devicearray.h:221-237).
             for (int i = ia; i < ib; i++) {
-                if (i >= i0 && i < i1) continue;
-                mx = max(mx, abs_bits(a.dst[(long long)i * G.sx + bjk]));
+                const unsigned m = (i >= i0 && i < i1) ? (ins & ~inr) : ins;
+                if (!m) continue;
+                const T* rp = a.dst + (long long)i * G.sx + bjk;
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    if ((m >> e) & 1u) mx = max(mx, abs_bits(rp[e]));
             }
         }
         if (i0 < i1) {
-            // src may alias dst (in-place Gauss-Seidel): reads go through ldg() and only touch
-            // points of the colour this pass does not write.
+            // src may alias dst (in-place Gauss-Seidel): every value a thread reads belongs to
+            // the colour this pass does not write, or to its own vector.
             const T* src = a.src;
             const T* f = a.f;
             const T two_h = a.two_h;
-            // u(i0-1): a stored value or the west ghost  -2h*gW + u(1)
-            T vc = ldg(src + (long long)i0 * G.sx + bjk);
-            T vm;
-            if (i0 > 0) vm = ldg(src + (long long)(i0 - 1) * G.sx + bjk);
-            else vm = (-two_h) * ldg(a.F.g[F_WEST] + (long long)j * G.nz + k) + ldg(src + G.sx + bjk);
-            T vm_old = vm;  // u(i-1) before this sweep touched it (mirror of the east ghost)
+            const T m2h = -two_h;
+            T vm[V], vc[V], vp[V], vpp[V], fc[V], fn[V], vmo[V];
+            ldv(vc, src + (long long)i0 * G.sx + bjk);
+            if (i0 > 0) {
+                ldv(vm, src + (long long)(i0 - 1) * G.sx + bjk);
+            } else {  // west ghost  -2h*gW + u(1)
+                T v1[V];
+                ldv(v1, src + G.sx + bjk);
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    vm[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_WEST] + (long long)j * G.nz + kb + e) + v1[e] : T(0);
+            }
+#pragma unroll
+            for (int e = 0; e < V; e++) vmo[e] = vm[e];
+            if (i0 + 1 < G.nx) ldv(vp, src + (long long)(i0 + 1) * G.sx + bjk);
+            ldv(fc, f + (long long)i0 * G.sx + bjk);
             for (int i = i0; i < i1; i++) {
                 const long long p = (long long)i * G.sx + bjk;
-                T vp;
-                if (i + 1 < G.nx) vp = ldg(src + p + G.sx);
-                else vp = two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + k) + vm_old;
-                bool active = true;
-                if (OP == OP_GS) active = ((i + j + k + G.poff) & 1) == a.colour;
-                if (OP == OP_GS_COLUMN) active = ((j + k + G.poff) & 1) == a.colour;
-                T vc_old = vc;
-                if (active) {
-                    T ym, yp, zm, zp;
-                    if (j > 0) ym = ldg(src + p - G.sy);
-                    else ym = (-two_h) * ldg(a.F.g[F_SOUTH] + (long long)i * G.nz + k) + ldg(src + p + G.sy);
-                    if (j < G.ny - 1) yp = ldg(src + p + G.sy);
-                    else yp = two_h * ldg(a.F.g[F_NORTH] + (long long)i * G.nz + k) + ldg(src + p - G.sy);
-                    if (k > 0) zm = ldg(src + p - 1);
-                    else zm = (-two_h) * ldg(a.F.g[F_BOTTOM] + (long long)i * G.ny + j) + ldg(src + p + 1);
-                    if (k < G.nz - 1) zp = ldg(src + p + 1);
-                    else zp = two_h * ldg(a.F.g[F_TOP] + (long long)i * G.ny + j) + ldg(src + p - 1);
-                    const T sum = vm + vp + ym + yp + zm + zp;
-                    if (OP == OP_RESIDUAL) {
-                        const T r = residual_expr(ldg(f + p), sum, vc, a.hsq);
-                        a.dst[p] = r;
-                        mx = max(mx, abs_bits(r));
+                if (i + 1 < i1) {
+                    if (i + 2 < G.nx) ldv(vpp, src + p + 2 * G.sx);
+                    ldv(fn, f + p + G.sx);
+                }
+                if (i + 1 == G.nx) {  // east ghost  2h*gE + u(nx-2), from before this sweep
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + kb + e) + vmo[e]
+                                                  : T(0);
+                }
+                unsigned act = inr;
+                if (OP == OP_GS || OP == OP_GS_COLUMN) {
+                    const int base = (OP == OP_GS ? i : 0) + j + kb + G.poff;
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if (((base + e) & 1) != a.colour) act &= ~(1u << e);
+                }
+                T cur[V];
+#pragma unroll
+                for (int e = 0; e < V; e++) cur[e] = vc[e];
+                if (act) {
+                    T ym[V], yp[V];
+                    if (j > 0) {
+                        ldv(ym, src + p - G.sy);
+                    } else {  // south ghost  -2h*gS + u(j=1)
+                        T w[V];
+                        ldv(w, src + p + G.sy);
+#pragma unroll
+                        for (int e = 0; e < V; e++)
+                            ym[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_SOUTH] + (long long)i * G.nz + kb + e) + w[e]
+                                                      : T(0);
+                    }
+                    if (j < G.ny - 1) {
+                        ldv(yp, src + p + G.sy);
+                    } else {  // north ghost  2h*gN + u(j=ny-2)
+                        T w[V];
+                        ldv(w, src + p - G.sy);
+#pragma unroll
+                        for (int e = 0; e < V; e++)
+                            yp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_NORTH] + (long long)i * G.nz + kb + e) + w[e]
+                                                      : T(0);
+                    }
+                    const T left = kb > 0 ? ldg(src + p - 1) : T(0);
+                    const T right = kb + V < G.nz ? ldg(src + p + V) : T(0);
+#pragma unroll
+                    for (int e = 0; e < V; e++) {
+                        if (!((act >> e) & 1u)) continue;
+                        const int k = kb + e;
+                        const T below = e > 0 ? vc[e - 1] : left;   // u(k-1)
+                        const T above = e < V - 1 ? vc[e + 1] : right;  // u(k+1)
+                        T zm, zp;
+                        if (k > 0) zm = below;
+                        else zm = m2h * ldg(a.F.g[F_BOTTOM] + (long long)i * G.ny + j) + vc[1];  // -2h*gB + u(1)
+                        if (k < G.nz - 1) zp = above;
+                        else zp = two_h * ldg(a.F.g[F_TOP] + (long long)i * G.ny + j) + below;  // 2h*gT + u(nz-2)
+                        const T sum = vm[e] + vp[e] + ym[e] + yp[e] + zm + zp;
+                        if (OP == OP_RESIDUAL) {
+                            const T r = residual_expr(fc[e], sum, vc[e], a.hsq);
+                            cur[e] = r;
+                            mx = max(mx, abs_bits(r));
+                        } else {
+                            // jacobi.h:59-61 / gaussseidel.h:43-45:
+                            //   u = one_omega*v + omega_sixth*(sum - hsq*f)
+                            cur[e] = a.one_omega * vc[e] + a.omega_sixth * (sum - a.hsq * fc[e]);
+                        }
+                    }
+                    T* out = a.dst + p;
+                    if (OP == OP_GS || OP == OP_GS_COLUMN) {
+                        // the whole vector is this thread's; untouched entries keep their value
+                        stv(out, cur);
+                    } else if (act == full) {
+                        stv(out, cur);
                     } else {
-                        // jacobi.h:59-61 / gaussseidel.h:43-45:
-                        //   u = one_omega*v + omega_sixth*(sum - hsq*f)
-                        const T nv = a.one_omega * vc + a.omega_sixth * (sum - a.hsq * ldg(f + p));
-                        a.dst[p] = nv;
-                        vc = nv;
+#pragma unroll
+                        for (int e = 0; e < V; e++)
+                            if ((act >> e) & 1u) out[e] = cur[e];
                     }
                 }
-                vm_old = vc_old;
-                vm = vc;
-                vc = vp;
+#pragma unroll
+                for (int e = 0; e < V; e++) {
+                    vmo[e] = vc[e];
+                    // in place (Gauss-Seidel) the register copy follows memory; Jacobi and the
+                    // residual keep marching over the source iterate
+                    vm[e] = (OP == OP_GS || OP == OP_GS_COLUMN) ? cur[e] : vc[e];
+                    vc[e] = vp[e];
+                    vp[e] = vpp[e];
+                    fc[e] = fn[e];
+                }
             }
         }
     }
@@ -291,31 +419,68 @@ __device__ __forceinline__ T half_sum(T a, T b) {
 
 template <typename T, bool ADD>
 __global__ void __launch_bounds__(256) k_prolong(const T* __restrict__ uc, Geom Gc, T* u, T* r, Geom Gf) {
-    const long long n = (long long)Gf.nx * Gf.ny * Gf.nz;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t % Gf.nz);
-        const long long q = t / Gf.nz;
-        const int j = (int)(q % Gf.ny);
-        const int i = (int)(q / Gf.ny);
-        const int ic = i >> 1, jc = j >> 1, kc = k >> 1;
-        auto C = [&](int x, int y, int z) -> T { return ldg(uc + x * Gc.sx + y * Gc.sy + z); };
-        auto X = [&](int y, int z) -> T {  // value at (i, 2y, 2z) after the x pass
-            T v = C(ic, y, z);
-            if (i & 1) v = half_sum(v, C(ic + 1, y, z));
-            return v;
-        };
-        auto Y = [&](int z) -> T {  // value at (i, j, 2z) after the y pass
-            if (j & 1) return half_sum(X(jc, z), X(jc + 1, z));
-            return X(jc, z);
-        };
-        const T e = (k & 1) ? half_sum(Y(kc), Y(kc + 1)) : Y(kc);
-        const long long p = (long long)i * Gf.sx + (long long)j * Gf.sy + k;
-        if (ADD) {
-            u[p] = u[p] + e;
-            const bool inside = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1 && k >= Gf.z0 && k < Gf.z1;
-            if (!inside) r[p] = e;
+    // one thread: a V-vector of fine k points of row (i = blockIdx.y, j)
+    constexpr int V = VecT<T>::V;
+    const int nv = (Gf.nz + V - 1) / V;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Gf.ny * nv) return;
+    const int i = blockIdx.y;
+    const int j = t / nv;
+    const int kb = (t - j * nv) * V;  // even
+    const int ic = i >> 1, jc = j >> 1;
+    auto C = [&](int x, int y, int z) -> T { return ldg(uc + x * Gc.sx + y * Gc.sy + z); };
+    auto X = [&](int y, int z) -> T {  // value at (i, 2y, 2z) after the x pass
+        T v = C(ic, y, z);
+        if (i & 1) v = half_sum(v, C(ic + 1, y, z));
+        return v;
+    };
+    auto Y = [&](int z) -> T {  // value at (i, j, 2z) after the y pass
+        if (j & 1) return half_sum(X(jc, z), X(jc + 1, z));
+        return X(jc, z);
+    };
+    constexpr int NQ = V / 2 + 1;
+    T yv[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        const int z = (kb >> 1) + q;
+        yv[q] = z < Gc.nz ? Y(z) : T(0);
+    }
+    T ev[V];
+    unsigned ins = 0u, inside = 0u;
+    const bool ijin = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1;
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const int k = kb + e;
+        // z pass: odd k averages the two neighbouring even-k values
+        ev[e] = (e & 1) ? half_sum(yv[e >> 1], yv[(e >> 1) + 1]) : yv[e >> 1];
+        if (k < Gf.nz) ins |= 1u << e;
+        if (ijin && k >= Gf.z0 && k < Gf.z1) inside |= 1u << e;
+    }
+    const long long p = (long long)i * Gf.sx + (long long)j * Gf.sy + kb;
+    const unsigned full = (1u << V) - 1u;
+    if (ADD) {
+        if (ins == full) {
+            T uv[V];
+            ldv_rw(uv, u + p);
+#pragma unroll
+            for (int e = 0; e < V; e++) uv[e] = uv[e] + ev[e];
+            stv(u + p, uv);
         } else {
-            r[p] = e;
+#pragma unroll
+            for (int e = 0; e < V; e++)
+                if ((ins >> e) & 1u) u[p + e] = u[p + e] + ev[e];
+        }
+        const unsigned rm = ins & ~inside;
+#pragma unroll
+        for (int e = 0; e < V; e++)
+            if ((rm >> e) & 1u) r[p + e] = ev[e];
+    } else {
+        if (ins == full) {
+            stv(r + p, ev);
+        } else {
+#pragma unroll
+            for (int e = 0; e < V; e++)
+                if ((ins >> e) & 1u) r[p + e] = ev[e];
         }
     }
 }

@@ -1,0 +1,130 @@
+// mgp_drivers.cpp -- the reference's example executables (drivers/*.cpp of
+// eljens/multigrid-poisson) on the B200 engine, one source compiled six ways with
+// -DMGP_APP_<NAME>:
+//   FCYCLE / VCYCLE  Injection + Trilinear + Jacobi, BC {N,N,N,N,D,D}, nsmooth 4, F- or
+//                    V-cycle; "-stats" appends the reference's 7-column row
+//                    (drivers/fcycle.cpp:21-54).
+//   MIXED            Injection + Jacobi, BC {N,N,N,N,D,D}, V-cycle nsmooth 6, prints the max
+//                    error against ufun and appends the 10-column row (drivers/mixed.cpp).
+//   DIRICHLET        as MIXED with all faces Dirichlet.
+//   NEUMANN          as MIXED with every face requested Neumann.
+//   GAUSSSEIDEL      FullWeighting + red-black SOR (omega 0.7), BC {N,N,N,N,D,D}.
+// Command-line flags are the reference's (src/parser.cpp): -x -y -z -l/-levels -maxiter
+// -tol/-tolerance -length -s/-save -stats <file>.  One solver runs on one GPU
+// (device 0, or $MGP_DEVICE).
+#include <algorithm>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+
+#include "libpoisson.h"
+#include "parser.h"
+
+using namespace Poisson;
+
+#if defined(MGP_APP_FCYCLE) || defined(MGP_APP_VCYCLE)
+int main(int argc, char* argv[]) {
+    Settings settings = parser(argc, argv);
+    if (const char* d = std::getenv("MGP_DEVICE")) settings.dev = std::atoi(d);
+    BoundaryCondition BC{NEUMANN, NEUMANN, NEUMANN, NEUMANN, DIRICHLET, DIRICHLET};
+    PoissonSolver<double_t, Injection, TrilinearInterpolation, Jacobi> solver(settings, BC);
+    solver.init();
+    solver.verbose(true);
+    solver.to_device();
+#if defined(MGP_APP_FCYCLE)
+    const char* cyc = "fcycle";
+    const char* what = "Fcycles";
+#else
+    const char* cyc = "vcycle";
+    const char* what = "Fcycles";  // the reference's vcycle driver prints the same word
+#endif
+    solver.solve(cyc, 4);
+    cout << "It took " << solver.solve_time() << " seconds to run ";
+    cout << solver.solve_iterations() << " " << what << endl;
+    if (settings.print_result) {
+        solver.to_host();
+        solver.save_all("results/u_vcycle.vtk", "results/f_vcycle.vtk", "results/r_vcycle.vtk");
+    }
+    if (settings.write_final_stats) {
+        ofstream out("results/" + settings.stats_file, ios::app);
+        out << "#    seconds     rel_res domain_size     spacing     maxiter     lengthx      levels" << endl;
+        out << setw(12) << solver.solve_time();
+        out << setw(12) << solver.relative_residual();
+        out << setw(12) << settings.dims[0] * settings.dims[1] * settings.dims[2];
+        out << setw(12) << settings.h;
+        out << setw(12) << solver.solve_iterations();
+        out << setw(12) << settings.lengthx;
+        out << setw(12) << settings.levels;
+        out << endl;
+    }
+    return EXIT_SUCCESS;
+}
+
+#else  // MIXED / DIRICHLET / NEUMANN / GAUSSSEIDEL
+
+#if defined(MGP_APP_DIRICHLET)
+static const BoundaryCondition kBC{DIRICHLET, DIRICHLET, DIRICHLET, DIRICHLET, DIRICHLET, DIRICHLET};
+#elif defined(MGP_APP_NEUMANN)
+static const BoundaryCondition kBC{NEUMANN, NEUMANN, NEUMANN, NEUMANN, NEUMANN, NEUMANN};
+#else
+static const BoundaryCondition kBC{NEUMANN, NEUMANN, NEUMANN, NEUMANN, DIRICHLET, DIRICHLET};
+#endif
+
+int main(int argc, char* argv[]) {
+    int ndev = 0;
+    mgp_device_count(&ndev);
+    Settings settings = parser(argc, argv);
+    if (const char* d = std::getenv("MGP_DEVICE")) settings.dev = std::atoi(d);
+    BoundaryCondition BC = kBC;
+    int_t dev_shape[3] = {1, 1, 1};
+    cout << "MG running on 1 host thread and " << 1 << " of " << ndev << " devices" << endl;
+#if defined(MGP_APP_GAUSSSEIDEL)
+    PoissonSolver<double_t, FullWeighting, TrilinearInterpolation, GaussSeidel> solver(dev_shape, settings, BC);
+#else
+    PoissonSolver<double_t, Injection, TrilinearInterpolation, Jacobi> solver(dev_shape, settings, BC);
+#endif
+    solver.init();
+    solver.verbose(true);
+    solver.to_device();
+#if defined(MGP_APP_GAUSSSEIDEL)
+    solver.solve("vcycle", 6, 0.7);
+#else
+    solver.solve("vcycle", 6);
+#endif
+    cout << "It took " << solver.solve_time() << " seconds to run ";
+    cout << solver.solve_iterations() << " Fcycles" << endl;
+    solver.to_host();
+    if (settings.print_result)
+        solver.save_all(0, "results/u_0.vtk", "results/f_0.vtk", "results/r_0.vtk");
+    // maximal error against the analytic solution over the shape points (drivers/mixed.cpp:66-102)
+    const DeviceArray<double_t>& u = solver.get_solution(0);
+    double_t maxerr = 0.0;
+    for (int_t i = 0; i < u.shape[0]; i++)
+        for (int_t j = 0; j < u.shape[1]; j++)
+            for (int_t k = 0; k < u.shape[2]; k++) {
+                const double_t ut = ufun(settings.origin[0] + ((double_t)i) * settings.h,
+                                         settings.origin[1] + ((double_t)j) * settings.h,
+                                         settings.origin[2] + ((double_t)k) * settings.h);
+                maxerr = std::max(maxerr, std::abs(u.at[u.idx(i, j, k)] - ut));
+            }
+    cout << "Maximal error: " << setw(8) << maxerr << endl;
+    if (settings.write_final_stats) {
+        ofstream out(settings.stats_file, ios::app);
+        out << "#    seconds     abs_err     rel_res domain_size     spacing     maxiter     lengthx      levels     "
+               "threads     devices"
+            << endl;
+        out << setw(12) << solver.solve_time();
+        out << setw(12) << maxerr;
+        out << setw(12) << solver.relative_residual();
+        out << setw(12) << settings.dims[0] * settings.dims[1] * settings.dims[2];
+        out << setw(12) << settings.h;
+        out << setw(12) << solver.solve_iterations();
+        out << setw(12) << settings.lengthx;
+        out << setw(12) << settings.levels;
+        out << setw(12) << 1;
+        out << setw(12) << 1;
+        out << endl;
+    }
+    return EXIT_SUCCESS;
+}
+#endif

@@ -33,6 +33,40 @@ def needs_build() -> bool:
     return any(p.stat().st_mtime > t for p in sources())
 
 
+DRIVERS = ROOT / "drivers"
+FACADE = ROOT / "poisson"
+APPS = ("fcycle", "vcycle", "mixed", "dirichlet", "neumann", "gaussseidel")
+
+
+def driver_path(app: str, problem: int) -> Path:
+    return DRIVERS / "bin" / f"{app}_p{problem}"
+
+
+def build_drivers(problems=(1, 2, 3), force: bool = False) -> list:
+    """The reference's six example executables over the C++ facade, one per test problem
+    (compile-time PROBLEMn, as the reference's Makefile selects it)."""
+    build()
+    out = []
+    deps = [DRIVERS / "mgp_drivers.cpp", DRIVERS / "problems.cpp", LIB] + sorted(FACADE.glob("*.h"))
+    newest = max(p.stat().st_mtime for p in deps)
+    (DRIVERS / "bin").mkdir(exist_ok=True)
+    cxx = os.environ.get("CXX", "g++")
+    for prob in problems:
+        for app in APPS:
+            exe = driver_path(app, prob)
+            if not force and exe.exists() and exe.stat().st_mtime >= newest:
+                out.append(exe)
+                continue
+            tmp = exe.with_suffix(".tmp")
+            subprocess.check_call([cxx, "-std=c++17", "-O2", f"-DMGP_APP_{app.upper()}", f"-DPROBLEM{prob}",
+                                   f"-I{FACADE}", f"-I{INCLUDE}", str(DRIVERS / "mgp_drivers.cpp"),
+                                   str(DRIVERS / "problems.cpp"), f"-L{PKG}", "-lmgp",
+                                   "-Wl,-rpath,$ORIGIN/../../mgp", "-o", str(tmp)])
+            os.replace(tmp, exe)
+            out.append(exe)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return LIB

@@ -21,7 +21,7 @@ CONFIGS = [
     # dims, levels, bc (N S E W T B), restriction, relaxation
     ((17, 9, 9), 2, (1, 1, 1, 1, 0, 0), "fw", "jacobi"),
     ((33, 17, 9), 3, (0, 0, 1, 1, 1, 0), "inj", "jacobi"),
-    ((33, 17, 17), 3, (0, 0, 1, 1, 1, 0), "fw", "gs"),
+    ((33, 17, 17), 3, (0, 0, 1, 1, 1, 1), "fw", "gs"),  # top/bottom requested N: padded z odd
     ((17, 17, 17), 3, (0, 0, 0, 0, 0, 0), "inj", "gs"),
     ((17, 9, 17), 2, (1, 0, 0, 0, 0, 0), "inj", "gs"),  # padded y even: column order
     ((65, 33, 33), 4, (1, 1, 1, 1, 0, 0), "fw", "jacobi"),
@@ -46,12 +46,20 @@ def pair(mgp, cfg, seed):
     return o, e
 
 
+def live_faces(o, level):
+    """Faces whose data the cycle reads at this level: every face on the finest level, the
+    Neumann faces below it.  Coarse Dirichlet face arrays are never read; the reference
+    re-zeroes them on every visit (dirichlet.h:101-107) while the engine keeps them zero
+    from allocation, so they are not compared after a random start."""
+    return [fc for fc in range(6) if level == 0 or o.face_types[fc] == 1]
+
+
 def check_all(o, e, fields=("u", "f", "r"), faces=True):
     for l in range(o.levels):
         for name in fields:
             assert_field_equal(o, e, name, l)
         if faces:
-            for fc in range(6):
+            for fc in live_faces(o, l):
                 assert_face_equal(o, e, fc, l)
 
 
@@ -138,8 +146,7 @@ def test_cycle_bit_exact(mgp_mod, gpu_ready, ci, cycle):
     for l in range(o.levels):
         assert_field_equal(o, e, "u", l)
         assert_field_equal(o, e, "f", l)
-    for fc in range(6):
-        for l in range(o.levels):
+        for fc in live_faces(o, l):
             assert_face_equal(o, e, fc, l)
 
 
@@ -174,6 +181,14 @@ def test_solve_matches_reference_golden(mgp_mod, gpu_ready, name):
     cfg = golden_cfg(SOLVES[name])
     o = make_oracle(cfg)
     o.init_problem(cfg["problem"], tuple(cfg["origin"]))
+    pad_z = cfg["dims"][2] + (cfg["bc"][4] != 0) + (cfg["bc"][5] != 0)
+    if cfg["relaxation"] == "gs" and pad_z % 2 == 0:
+        # degenerate red-black colouring: the engine refuses the layout (the reference's
+        # parallel result depends on thread timing; the fixture is its one-thread run)
+        with pytest.raises(mgp_mod.MgpError) as ei:
+            make_engine(mgp_mod, cfg)
+        assert ei.value.status == mgp_mod.ERR_UNSUPPORTED
+        return
     e, st = run_engine_solve(mgp_mod, cfg, o)
     u = e.download("u", 0)[e.level[0].interior]
     r = e.download("r", 0)[e.level[0].interior]
@@ -226,7 +241,10 @@ def test_operator_matches_reference_golden(mgp_mod, gpu_ready, name):
             got = e.download(f, l)[lv.interior]
             want = case[f"out/L{l}_{f}"][lv.interior]
             assert np.array_equal(got, want), (name, f, l, float(np.max(np.abs(got - want))))
+        kinds = e.level[l].face_kind
         for fc, fn in enumerate(FACES):
+            if l > 0 and kinds[fc] == 0 and m["ops"][0].split(":")[0] in ("vcycle", "fcycle"):
+                continue  # coarse Dirichlet data: never read, see live_faces()
             assert np.array_equal(e.download_face(fc, l), case[f"out/L{l}_{fn}"]), (name, fn, l)
 
 
