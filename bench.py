@@ -87,7 +87,7 @@ class ClockSampler:
         try:
             self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.tmp,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.tmp,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -285,8 +285,8 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mgp", choices=["mgp", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -304,14 +304,18 @@ def main():
     ps.to_device()
     eng = ps.engine
     stream = torch.cuda.ExternalStream(eng.stream_handle, device=f"cuda:{local}")
-    # warm-up (captures and instantiates the CUDA graph)
-    eng.set_iteration_limits(args.warmup, args.warmup, 0.0)
-    eng.solve("Fcycle", NSMOOTH)
-    eng.set_iteration_limits(args.steps, args.steps, 0.0)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(pg)
-    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        # warm-up (captures and instantiates the CUDA graph); the sampler's first readings
+        # land here, under load, before the timed region
+        eng.set_iteration_limits(args.warmup, args.warmup, 0.0)
+        eng.solve("Fcycle", NSMOOTH)
+        t_end = time.time() + 0.6
+        while time.time() < t_end:
+            eng.solve("Fcycle", NSMOOTH)
+        eng.set_iteration_limits(args.steps, args.steps, 0.0)
+        barrier(pg)
+        torch.cuda.synchronize()
         ev0.record(stream)
         st = eng.solve("Fcycle", NSMOOTH)
         ev1.record(stream)

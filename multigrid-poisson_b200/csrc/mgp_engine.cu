@@ -147,6 +147,17 @@ int check_launch(mgp_solver* s) {
     return MGP_OK;
 }
 
+// x/hsq equals x*(1/hsq) bit for bit when hsq is a power of two (scaling by 2^k is exact);
+// the kernels then multiply instead of dividing.
+template <typename T>
+void hsq_terms(T hsq, T& inv, int& pow2) {
+    int ex = 0;
+    const double m = std::frexp((double)hsq, &ex);
+    pow2 = (m == 0.5) && std::isfinite((double)hsq) && std::isnormal((double)hsq);
+    inv = pow2 ? (T)(1.0 / (double)hsq) : T(0);
+    if (pow2 && !std::isnormal((double)inv)) pow2 = 0;
+}
+
 // ---- stencil launches -------------------------------------------------------------------
 template <typename T, int OP>
 int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, int colour, unsigned long long* norm) {
@@ -163,6 +174,7 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     a.hsq = (T)(L.h * L.h);
     a.one_omega = (T)(1.0 - omega);
     a.omega_sixth = (T)(omega / 6.0);
+    hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
     a.colour = colour;
     a.norm = norm;
     constexpr int V = VecT<T>::V;
@@ -236,28 +248,19 @@ int restrict_t(mgp_solver* s, int l, bool zero_coarse_u) {
 }
 
 template <typename T>
+BcRestrictArgs<T> bc_args(mgp_solver* s, int l, bool* any);
+
+template <typename T>
 int restrict_bc_t(mgp_solver* s, int l) {
     bool any = false;
-    BcRestrictArgs<T> a;
-    LevelState& F = s->lv[l];
+    BcRestrictArgs<T> a = bc_args<T>(s, l, &any);
+    // Dirichlet faces: coarse g = 0 (dirichlet.h:101-107).  Coarse Dirichlet arrays are
+    // zero from allocation and nothing in a cycle writes them, so there is nothing to launch.
+    if (!any) return MGP_OK;
     LevelState& C = s->lv[l + 1];
     long long nmax = 1;
-    for (int f = 0; f < 6; f++) {
-        a.gf[f] = (const T*)F.face[f];
-        a.gc[f] = (T*)C.face[f];
-        a.vf[f] = face_view(F.face_shape[f]);
-        a.vc[f] = face_view(C.face_shape[f]);
-        a.neumann[f] = s->face_kind[f] == MGP_NEUMANN;
-        any |= a.neumann[f] != 0;
+    for (int f = 0; f < 6; f++)
         nmax = std::max(nmax, (long long)(C.face_shape[f][0] * C.face_shape[f][1] * C.face_shape[f][2]));
-    }
-    // Dirichlet faces: coarse g = 0 (dirichlet.h:101-107).  Coarse Dirichlet arrays are
-    // zero from allocation and nothing else writes them, so there is nothing to launch.
-    if (!any) return MGP_OK;
-    a.u = (const T*)u_ptr(s, l);
-    a.Gf = F.G;
-    a.h = (T)F.h;
-    a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
     dim3 grid((unsigned)std::max(1ll, std::min((nmax + kThreads - 1) / kThreads, 4096ll)), 6);
     k_restrict_bc<T><<<grid, kThreads, 0, s->stream>>>(a);
     return check_launch(s);
@@ -296,13 +299,77 @@ int norm_t(mgp_solver* s, const void* a, int l, unsigned long long* out) {
     return check_launch(s);
 }
 
-// coarse-grid correction set-up shared by both cycles (vcycle.h:34-76, fcycle.h:130-172)
+template <typename T>
+BcRestrictArgs<T> bc_args(mgp_solver* s, int l, bool* any) {
+    BcRestrictArgs<T> a;
+    LevelState& F = s->lv[l];
+    LevelState& C = s->lv[l + 1];
+    *any = false;
+    for (int f = 0; f < 6; f++) {
+        a.gf[f] = (const T*)F.face[f];
+        a.gc[f] = (T*)C.face[f];
+        a.vf[f] = face_view(F.face_shape[f]);
+        a.vc[f] = face_view(C.face_shape[f]);
+        a.neumann[f] = s->face_kind[f] == MGP_NEUMANN;
+        *any |= a.neumann[f] != 0;
+    }
+    a.u = (const T*)u_ptr(s, l);
+    a.Gf = F.G;
+    a.h = (T)F.h;
+    a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
+    return a;
+}
+
+// Coarse-grid correction set-up (vcycle.h:34-76, fcycle.h:130-172) in one launch:
+// residual(l) -> restrict -> u_{l+1}.init_zero(), plus the Neumann face restriction.
 template <typename T>
 int coarse_setup_t(mgp_solver* s, int l) {
-    CKS(residual_t<T>(s, l, nullptr));
-    CKS(restrict_t<T>(s, l, /*zero_coarse_u=*/true));  // restrict + u_{l+1}.init_zero()
-    CKS(restrict_bc_t<T>(s, l));
-    return MGP_OK;
+    LevelState& F = s->lv[l];
+    LevelState& C = s->lv[l + 1];
+    constexpr int V = VecT<T>::V;
+    RRArgs<T> a;
+    a.Gf = F.G;
+    a.Gc = C.G;
+    a.u = (const T*)u_ptr(s, l);
+    a.f = (const T*)F.f;
+    a.r = (const T*)F.r;
+    a.fc = (T*)C.f;
+    a.uc = (T*)u_ptr(s, l + 1);
+    a.F = faces_of<T>(s, l);
+    a.two_h = (T)(2.0 * F.h);
+    a.hsq = (T)(F.h * F.h);
+    hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
+    a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
+    // coarse tile: tkc points along k (2*tkc a multiple of V keeps rows aligned), tjc rows
+    int tkc = V == 2 ? 31 : 30;
+    if (C.G.nz < tkc) tkc = (V == 2) ? C.G.nz : (C.G.nz + 1) / 2 * 2;
+    const int tkv = (2 * tkc + V) / V;
+    const int tjc = std::max(1, std::min(C.G.ny, (256 / tkv - 1) / 2));
+    const int rows = 2 * tjc + 1;
+    a.tkc = tkc;
+    a.tjc = tjc;
+    a.tiles_j = (C.G.ny + tjc - 1) / tjc;
+    a.tiles_k = (C.G.nz + tkc - 1) / tkc;
+    const int tiles = a.tiles_j * a.tiles_k;
+    const int target = sm_count(s->device) * 8;
+    const int chunks = std::max(1, std::min((target + tiles - 1) / tiles, C.G.nx));
+    a.ci = (C.G.nx + chunks - 1) / chunks;
+    const int nchunks = (C.G.nx + a.ci - 1) / a.ci;
+    a.main_blocks = tiles * nchunks;
+    bool any = false;
+    a.bc = bc_args<T>(s, l, &any);
+    int extra = 0;
+    a.bc_blocks_per_face = 1;
+    if (any) {
+        long long nmax = 1;
+        for (int f = 0; f < 6; f++)
+            nmax = std::max(nmax, (long long)(C.face_shape[f][0] * C.face_shape[f][1] * C.face_shape[f][2]));
+        a.bc_blocks_per_face = (int)std::max(1ll, std::min(64ll, (nmax + tkv * rows - 1) / (tkv * rows)));
+        extra = 6 * a.bc_blocks_per_face;
+    }
+    const size_t smem = (size_t)3 * rows * (tkv * V) * sizeof(T);
+    k_resid_restrict<T><<<a.main_blocks + extra, dim3(tkv, rows), smem, s->stream>>>(a);
+    return check_launch(s);
 }
 
 template <typename T>

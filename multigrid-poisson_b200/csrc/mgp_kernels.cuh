@@ -88,17 +88,26 @@ struct StencilArgs {
     T hsq;         // h*h (T)
     T one_omega;   // 1-omega (T)
     T omega_sixth; // omega/6 (T)
+    T inv_hsq;     // 1/hsq, used only when hsq is a power of two (exact)
+    int hsq_pow2;
     int colour;    // GS colour (0 red: idx%2==0, 1 black)
     int ichunk;    // planes per block
     unsigned long long* norm;  // residual: max |r| over the whole shape (nullptr: none)
 };
 
-// Residual with the reference's promotions: f - (sum - 6.0*u)/hsq (include/residual.h:70-72).
-__device__ __forceinline__ double residual_expr(double f, double sum, double u, double hsq) {
-    return f - (sum - 6.0 * u) / hsq;
+// Residual with the reference's promotions: f - (sum - 6.0*u)/hsq (include/residual.h:70-72);
+// T=float evaluates in double because of the double literal 6.0.
+template <typename T>
+__device__ __forceinline__ T residual_pt(T fv, T sum, T uc, T hsq, T inv_hsq, int pow2);
+template <>
+__device__ __forceinline__ double residual_pt(double fv, double sum, double uc, double hsq, double inv_hsq, int pow2) {
+    // dividing by a power of two and multiplying by its exact reciprocal round identically
+    return pow2 ? fv - (sum - 6.0 * uc) * inv_hsq : fv - (sum - 6.0 * uc) / hsq;
 }
-__device__ __forceinline__ float residual_expr(float f, float sum, float u, float hsq) {
-    return (float)((double)f - ((double)sum - 6.0 * (double)u) / (double)hsq);
+template <>
+__device__ __forceinline__ float residual_pt(float fv, float sum, float uc, float hsq, float inv_hsq, int pow2) {
+    const double t = (double)sum - 6.0 * (double)uc;
+    return (float)((double)fv - (pow2 ? t * (double)inv_hsq : t / (double)hsq));
 }
 
 // 16-byte vectors along k: 2 doubles or 4 floats per thread.  Rows are 64-byte aligned, so
@@ -268,7 +277,7 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
                         else zp = two_h * ldg(a.F.g[F_TOP] + (long long)i * G.ny + j) + below;  // 2h*gT + u(nz-2)
                         const T sum = vm[e] + vp[e] + ym[e] + yp[e] + zm + zp;
                         if (OP == OP_RESIDUAL) {
-                            const T r = residual_expr(fc[e], sum, vc[e], a.hsq);
+                            const T r = residual_pt(fc[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
                             cur[e] = r;
                             mx = max(mx, abs_bits(r));
                         } else {
@@ -370,10 +379,9 @@ struct BcRestrictArgs {
     bool fw;
 };
 
+// Work of one face: thread `tid` of `nthr` cooperating threads.
 template <typename T>
-__global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
-    const int fc = blockIdx.y;
-    if (!a.neumann[fc]) return;
+__device__ __forceinline__ void bc_restrict_face(const BcRestrictArgs<T>& a, int fc, long long tid, long long nthr) {
     const View vo = a.vc[fc];
     const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
     const int nxf = a.Gf.nx, nyf = a.Gf.ny, nzf = a.Gf.nz;
@@ -392,7 +400,7 @@ __global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
         c2 = T(-2.0);
         c1 = T(3.0 / 2.0);
     }
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = tid; t < n; t += nthr) {
         const int k = (int)(t % vo.n[2]);
         const long long q = t / vo.n[2];
         const int j = (int)(q % vo.n[1]);
@@ -403,6 +411,215 @@ __global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
         auto U = [&](int xx, int yy, int zz) -> T { return ldg(a.u + xx * a.Gf.sx + yy * a.Gf.sy + zz); };
         g -= (c1 * U(x, y, z) + c2 * U(x + ii, y + jj, z + kk) + c3 * U(x + iii, y + jjj, z + kkk)) / a.h;
         a.gc[fc][i * vo.s0 + j * vo.s1 + k] = g;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
+    const int fc = blockIdx.y;
+    if (!a.neumann[fc]) return;
+    bc_restrict_face(a, fc, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
+// ------------------------------------------------------------------------------------
+// Coarse-grid set-up in one pass (include/vcycle.h:34-76): the residual of level l is
+// formed plane by plane and never stored; each block keeps the last three residual planes
+// of its (j,k) tile in shared memory and, every second plane, restricts them into f_{l+1}
+// (Injection or FullWeighting, the reference's summation order) and zeroes u_{l+1}.
+// Blocks past `main_blocks` restrict the Neumann face data instead.
+//
+// Block = (tkv, 2*tjc+1) threads: one thread per fine (row, k-vector) of the tile.  The
+// tile covers fine rows 2*J0-1 .. 2*(J0+tjc)-1 and fine k from 2*K0-V, so every fine point a
+// coarse point of the tile reads is inside it.  Residual values at points outside the
+// relaxation bounds are the stored r (the reference restricts whatever r holds there).
+template <typename T>
+struct RRArgs {
+    Geom Gf, Gc;
+    const T* u;
+    const T* f;
+    const T* r;
+    T* fc;
+    T* uc;
+    Faces<T> F;
+    T two_h, hsq, inv_hsq;
+    int hsq_pow2;
+    int fw;
+    int tjc, tkc, ci;
+    int tiles_j, tiles_k, main_blocks, bc_blocks_per_face;
+    BcRestrictArgs<T> bc;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_resid_restrict(RRArgs<T> a) {
+    if ((int)blockIdx.x >= a.main_blocks) {
+        const int b = blockIdx.x - a.main_blocks;
+        const int fc = b / a.bc_blocks_per_face;
+        if (!a.bc.neumann[fc]) return;
+        const long long nthr = (long long)a.bc_blocks_per_face * blockDim.x * blockDim.y;
+        const long long tid = (long long)(b % a.bc_blocks_per_face) * blockDim.x * blockDim.y +
+                              threadIdx.y * blockDim.x + threadIdx.x;
+        bc_restrict_face(a.bc, fc, tid, nthr);
+        return;
+    }
+    constexpr int V = VecT<T>::V;
+    extern __shared__ __align__(16) unsigned char rr_smem[];
+    T* ring = reinterpret_cast<T*>(rr_smem);
+    const Geom& Gf = a.Gf;
+    const Geom& Gc = a.Gc;
+    const int TW = blockDim.x * V;
+    const int PE = blockDim.y * TW;  // elements of one residual plane tile
+    int b = blockIdx.x;
+    const int tj = b % a.tiles_j;
+    b /= a.tiles_j;
+    const int tk = b % a.tiles_k;
+    const int chunk = b / a.tiles_k;
+    const int J0 = tj * a.tjc, K0 = tk * a.tkc;
+    const int I0 = chunk * a.ci, I1 = min(Gc.nx, I0 + a.ci);
+    const int jf0 = 2 * J0 - 1, kf0 = 2 * K0 - V;
+    const int j = jf0 + (int)threadIdx.y;
+    const int kb = kf0 + (int)threadIdx.x * V;
+    unsigned ins = 0u, inr = 0u;
+    const bool jok = j >= 0 && j < Gf.ny;
+    const bool jin = j >= Gf.y0 && j < Gf.y1;
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const int k = kb + e;
+        if (jok && k >= 0 && k < Gf.nz) {
+            ins |= 1u << e;
+            if (jin && k >= Gf.z0 && k < Gf.z1) inr |= 1u << e;
+        }
+    }
+    const long long bjk = (long long)j * Gf.sy + kb;  // used only when ins != 0
+    const int ia = max(0, 2 * I0 - 1), ib = min(Gf.nx - 1, 2 * I1 - 1);
+    const T two_h = a.two_h, m2h = -a.two_h;
+    T vm[V], vc[V], vp[V], vpp[V], fcur[V], fn[V], vmo[V];
+    if (ins) {
+        ldv(vc, a.u + (long long)ia * Gf.sx + bjk);
+        if (ia > 0) {
+            ldv(vm, a.u + (long long)(ia - 1) * Gf.sx + bjk);
+        } else {
+            T v1[V];
+            ldv(v1, a.u + Gf.sx + bjk);
+#pragma unroll
+            for (int e = 0; e < V; e++)
+                vm[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_WEST] + (long long)j * Gf.nz + kb + e) + v1[e] : T(0);
+        }
+#pragma unroll
+        for (int e = 0; e < V; e++) vmo[e] = vm[e];
+        if (ia + 1 < Gf.nx) ldv(vp, a.u + (long long)(ia + 1) * Gf.sx + bjk);
+        ldv(fcur, a.f + (long long)ia * Gf.sx + bjk);
+    }
+    T* myslot = ring + threadIdx.y * TW + threadIdx.x * V;
+    for (int i = ia; i <= ib; i++) {
+        const long long p = (long long)i * Gf.sx + bjk;
+        if (ins) {
+            if (i < ib) {
+                if (i + 2 < Gf.nx) ldv(vpp, a.u + p + 2 * Gf.sx);
+                ldv(fn, a.f + p + Gf.sx);
+            }
+            if (i + 1 == Gf.nx) {
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * Gf.nz + kb + e) + vmo[e]
+                                              : T(0);
+            }
+            const unsigned act = (i >= Gf.x0 && i < Gf.x1) ? inr : 0u;
+            T val[V];
+            if (ins & ~act) {
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    val[e] = (((ins & ~act) >> e) & 1u) ? ldg(a.r + p + e) : T(0);
+            }
+            if (act) {
+                T ym[V], yp[V];
+                if (j > 0) {
+                    ldv(ym, a.u + p - Gf.sy);
+                } else {
+                    T w[V];
+                    ldv(w, a.u + p + Gf.sy);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        ym[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_SOUTH] + (long long)i * Gf.nz + kb + e) + w[e] : T(0);
+                }
+                if (j < Gf.ny - 1) {
+                    ldv(yp, a.u + p + Gf.sy);
+                } else {
+                    T w[V];
+                    ldv(w, a.u + p - Gf.sy);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        yp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_NORTH] + (long long)i * Gf.nz + kb + e) + w[e]
+                                                  : T(0);
+                }
+                const T left = kb > 0 ? ldg(a.u + p - 1) : T(0);
+                const T right = kb + V < Gf.nz ? ldg(a.u + p + V) : T(0);
+#pragma unroll
+                for (int e = 0; e < V; e++) {
+                    if (!((act >> e) & 1u)) continue;
+                    const int k = kb + e;
+                    const T below = e > 0 ? vc[e - 1] : left;
+                    const T above = e < V - 1 ? vc[e + 1] : right;
+                    const T zm = k > 0 ? below : m2h * ldg(a.F.g[F_BOTTOM] + (long long)i * Gf.ny + j) + vc[1];
+                    const T zp = k < Gf.nz - 1 ? above : two_h * ldg(a.F.g[F_TOP] + (long long)i * Gf.ny + j) + below;
+                    const T sum = vm[e] + vp[e] + ym[e] + yp[e] + zm + zp;
+                    val[e] = residual_pt(fcur[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
+                }
+            }
+            T* dst = myslot + (i % 3) * PE;
+#pragma unroll
+            for (int e = 0; e < V; e++) dst[e] = val[e];
+#pragma unroll
+            for (int e = 0; e < V; e++) {
+                vmo[e] = vc[e];
+                vm[e] = vc[e];
+                vc[e] = vp[e];
+                vp[e] = vpp[e];
+                fcur[e] = fn[e];
+            }
+        }
+        __syncthreads();
+        int I = -1;
+        if (i & 1) I = (i - 1) >> 1;
+        else if (i == Gf.nx - 1) I = i >> 1;
+        if (I >= I0 && I < I1) {
+            const int ii = 2 * I, im = max(0, ii - 1), ip = min(Gf.nx - 1, ii + 1);
+            const T* Pm = ring + (im % 3) * PE;
+            const T* P0 = ring + (ii % 3) * PE;
+            const T* Pp = ring + (ip % 3) * PE;
+            const int nthr = blockDim.x * blockDim.y;
+            for (int c = threadIdx.y * blockDim.x + threadIdx.x; c < a.tjc * a.tkc; c += nthr) {
+                const int J = J0 + c / a.tkc, K = K0 + c % a.tkc;
+                if (J >= Gc.ny || K >= Gc.nz) continue;
+                const int jj = 2 * J, jm = max(0, jj - 1), jp = min(Gf.ny - 1, jj + 1);
+                const int kk = 2 * K, km = max(0, kk - 1), kp = min(Gf.nz - 1, kk + 1);
+                const int rj = jj - jf0, rm = jm - jf0, rp = jp - jf0;
+                const int ck = kk - kf0, cm = km - kf0, cp = kp - kf0;
+                T out;
+                if (a.fw) {
+                    // FullWeighting::restrict_to order (fullweighting.h:76-109), k offset outermost
+                    auto A = [&](const T* P, int row, int col) -> double { return (double)P[row * TW + col]; };
+                    const double s_m = 1.0 * A(Pm, rm, cm) + 2.0 * A(Pm, rj, cm) + 1.0 * A(Pm, rp, cm) +
+                                       2.0 * A(P0, rm, cm) + 4.0 * A(P0, rj, cm) + 2.0 * A(P0, rp, cm) +
+                                       1.0 * A(Pp, rm, cm) + 2.0 * A(Pp, rj, cm) + 1.0 * A(Pp, rp, cm);
+                    T tmp = (T)s_m;
+                    const double s_0 = 2.0 * A(Pm, rm, ck) + 4.0 * A(Pm, rj, ck) + 2.0 * A(Pm, rp, ck) +
+                                       4.0 * A(P0, rm, ck) + 8.0 * A(P0, rj, ck) + 4.0 * A(P0, rp, ck) +
+                                       2.0 * A(Pp, rm, ck) + 4.0 * A(Pp, rj, ck) + 2.0 * A(Pp, rp, ck);
+                    tmp = (T)((double)tmp + s_0);
+                    const double s_p = 1.0 * A(Pm, rm, cp) + 2.0 * A(Pm, rj, cp) + 1.0 * A(Pm, rp, cp) +
+                                       2.0 * A(P0, rm, cp) + 4.0 * A(P0, rj, cp) + 2.0 * A(P0, rp, cp) +
+                                       1.0 * A(Pp, rm, cp) + 2.0 * A(Pp, rj, cp) + 1.0 * A(Pp, rp, cp);
+                    tmp = (T)((double)tmp + s_p);
+                    out = (T)((double)tmp / 64.0);
+                } else {
+                    out = P0[rj * TW + ck];  // injection.h:63
+                }
+                const long long o = (long long)I * Gc.sx + (long long)J * Gc.sy + K;
+                a.fc[o] = out;
+                a.uc[o] = T(0);
+            }
+        }
+        __syncthreads();
     }
 }
 

@@ -89,13 +89,15 @@ def make_solves(ref: RefRun) -> dict:
 OPS = {
     # name: (dims, levels, bc, restriction, relaxation, ops, nsmooth, omega)
     "jacobi_relax": ((17, 9, 9), 2, (N, N, N, N, N, D), "fw", "jacobi", ["relax:0"], 2, -1.0),
-    "gs_relax": ((17, 9, 9), 2, (D, D, N, N, N, D), "inj", "gs", ["relax:0"], 1, -1.0),
+    "gs_relax": ((17, 9, 9), 2, (D, D, N, N, N, N), "inj", "gs", ["relax:0"], 1, -1.0),
+    # degenerate colouring (padded z even); the engine refuses this layout
+    "gs_relax_degenerate": ((17, 9, 9), 2, (D, D, N, N, N, D), "inj", "gs", ["relax:0"], 1, -1.0),
     "gs_relax_column": ((9, 9, 9), 2, (N, D, D, D, D, D), "inj", "gs", ["relax:0"], 2, 1.1),
     "residual": ((17, 9, 9), 2, (N, N, N, N, N, D), "fw", "jacobi", ["residual:0"], 1, -1.0),
     "restrict_inj": ((17, 9, 9), 2, (N, N, N, N, D, D), "inj", "jacobi", ["restrict:0"], 1, -1.0),
     "restrict_fw": ((17, 9, 9), 2, (N, N, N, N, D, D), "fw", "jacobi", ["restrict:0"], 1, -1.0),
     "bc_restrict_fw": ((17, 9, 9), 2, (D, D, N, N, N, D), "fw", "jacobi", ["bcrestrict:0"], 1, -1.0),
-    "bc_restrict_inj": ((17, 9, 9), 2, (D, D, N, N, N, D), "inj", "gs", ["bcrestrict:0"], 1, -1.0),
+    "bc_restrict_inj": ((17, 9, 9), 2, (D, D, N, N, N, N), "inj", "gs", ["bcrestrict:0"], 1, -1.0),
     "prolong": ((17, 9, 9), 2, (N, N, N, N, D, D), "fw", "jacobi", ["prolong:0"], 1, -1.0),
     "prolong_add": ((17, 9, 9), 2, (D, D, N, N, N, D), "fw", "jacobi", ["prolong:0", "add:0"], 1, -1.0),
     "write_bc": ((9, 9, 9), 2, (D, D, N, D, D, D), "fw", "jacobi", ["writebc:0"], 1, -1.0),
