@@ -195,6 +195,45 @@ def kernel_roofline(mgp, ps, torch, stream, reps: int = 20):
     return sec, alg
 
 
+def run_kernels(args):
+    """Each level-0 operator of the workload timed alone (CUDA events on the engine's
+    stream, `args.steps` launches after 3 warm-up launches).  Also the small case for
+    profiler captures: the process holds one 513x257x129 hierarchy (~0.7 GB)."""
+    import torch
+
+    import mgp
+
+    ps = build_solver(mgp, 0, maxiter=1, pinned=False)
+    ps.to_device()
+    eng = ps.engine
+    stream = torch.cuda.ExternalStream(eng.stream_handle, device="cuda:0")
+    n = NDOF
+    nc = ((DIMS[0] >> 1) + 1) * ((DIMS[1] >> 1) + 1) * ((DIMS[2] >> 1) + 1)
+    ops = {  # name: (callable, algorithmic bytes per launch)
+        "jacobi_sweep": (lambda: eng.relax(0, -1.0, 1), 24.0 * n),
+        "residual": (lambda: eng.residual(0), 24.0 * n),
+        "restrict_fw": (lambda: eng.restrict(0), 8.0 * (n + nc)),
+        "prolong_add": (lambda: eng.prolong_add(0), 8.0 * (2 * n + nc)),
+    }
+    peak, kind = measured_peaks()
+    out = {}
+    for name, (fn, nbytes) in ops.items():
+        for _ in range(3):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        us = a.elapsed_time(b) * 1e3 / args.steps
+        gbs = nbytes / (us * 1e-6) / 1e9
+        out[name] = {"us": us, "algorithmic_bytes": nbytes, "GB/s": gbs, "frac": gbs / peak}
+    print(json.dumps({"kernels": out, "peak_gbs": peak, "peak_kind": kind, "workload": WORKLOAD}))
+    return 0
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -289,9 +328,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mgp", choices=["mgp", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels", action="store_true", help="time each level-0 kernel alone")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.kernels:
+        return run_kernels(args)
 
     world, rank, local, pg = dist_setup(args.gpus)
     import torch

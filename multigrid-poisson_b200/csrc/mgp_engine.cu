@@ -323,7 +323,7 @@ BcRestrictArgs<T> bc_args(mgp_solver* s, int l, bool* any) {
 // Coarse-grid correction set-up (vcycle.h:34-76, fcycle.h:130-172) in one launch:
 // residual(l) -> restrict -> u_{l+1}.init_zero(), plus the Neumann face restriction.
 template <typename T>
-int coarse_setup_t(mgp_solver* s, int l) {
+int coarse_setup_fused_t(mgp_solver* s, int l) {
     LevelState& F = s->lv[l];
     LevelState& C = s->lv[l + 1];
     constexpr int V = VecT<T>::V;
@@ -370,6 +370,17 @@ int coarse_setup_t(mgp_solver* s, int l) {
     const size_t smem = (size_t)3 * rows * (tkv * V) * sizeof(T);
     k_resid_restrict<T><<<a.main_blocks + extra, dim3(tkv, rows), smem, s->stream>>>(a);
     return check_launch(s);
+}
+
+// The three-kernel form: residual (r stored), restriction with u_{l+1} = 0 fused, Neumann
+// face restriction.
+template <typename T>
+int coarse_setup_t(mgp_solver* s, int l) {
+    if (s->desc.flags & MGP_FLAG_FUSED_SETUP) return coarse_setup_fused_t<T>(s, l);
+    CKS(residual_t<T>(s, l, nullptr));
+    CKS(restrict_t<T>(s, l, /*zero_coarse_u=*/true));
+    CKS(restrict_bc_t<T>(s, l));
+    return MGP_OK;
 }
 
 template <typename T>

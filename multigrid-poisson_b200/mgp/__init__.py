@@ -36,6 +36,7 @@ FIELD_U, FIELD_UPREV, FIELD_F, FIELD_R = range(4)
 FIELDS = ("u", "uprev", "f", "r")
 CYCLE_RELAXATION, CYCLE_V, CYCLE_F = 0, 1, 2
 FLAG_STRICT_BC = 1
+FLAG_FUSED_SETUP = 8
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,
@@ -174,7 +175,7 @@ class Solver:
 
     def __init__(self, dims, levels, h, bc=(DIRICHLET,) * 6, restriction=INJECTION, relaxation=GAUSSSEIDEL,
                  dtype=F64, maxiter=100, miniter=1, tolerance=1e-6, origin=(0.0, 0.0, 0.0), device=0,
-                 strict_bc=False):
+                 strict_bc=False, flags=0):
         L = lib()
         d = Desc()
         d.dims[:] = list(dims)
@@ -186,7 +187,7 @@ class Solver:
         d.relaxation = relaxation if isinstance(relaxation, int) else _RELAXATIONS[relaxation]
         d.dtype = dtype
         d.device = device
-        d.flags = FLAG_STRICT_BC if strict_bc else 0
+        d.flags = (FLAG_STRICT_BC if strict_bc else 0) | flags
         self._h = ctypes.c_void_p()
         _check(L.mgp_create(ctypes.byref(d), ctypes.byref(self._h)))
         self.desc = d

@@ -29,12 +29,12 @@ def make_oracle(cfg: dict) -> Oracle:
                   rlx_id(cfg["relaxation"]), cfg.get("strict_bc", False))
 
 
-def make_engine(mgp, cfg: dict, dtype=None, maxiter=None, tol=None):
+def make_engine(mgp, cfg: dict, dtype=None, maxiter=None, tol=None, flags=0):
     return mgp.Solver(cfg["dims"], cfg["levels"], cfg["h"], tuple(cfg["bc"]), rst_id(cfg["restriction"]),
                       rlx_id(cfg["relaxation"]), dtype if dtype is not None else mgp.F64,
                       maxiter if maxiter is not None else cfg.get("maxiter", 10), 1,
                       tol if tol is not None else cfg.get("tol", 0.0), tuple(cfg.get("origin", (0, 0, 0))),
-                      0, cfg.get("strict_bc", False))
+                      0, cfg.get("strict_bc", False), flags=flags)
 
 
 def randomize(o: Oracle, seed: int, lo=-1.0, hi=1.0):

@@ -150,6 +150,22 @@ def test_cycle_bit_exact(mgp_mod, gpu_ready, ci, cycle):
             assert_face_equal(o, e, fc, l)
 
 
+@pytest.mark.parametrize("ci", range(len(CONFIGS)))
+def test_fused_setup_cycle_bit_exact(mgp_mod, gpu_ready, ci):
+    """The one-kernel residual+restriction form of the coarse-grid set-up."""
+    cfg = cfg_of(CONFIGS[ci])
+    o = make_oracle(cfg)
+    randomize(o, 80 + ci)
+    e = make_engine(mgp_mod, cfg, flags=mgp_mod.FLAG_FUSED_SETUP)
+    push(o, e)
+    om = o.default_omega()
+    o.fcycle(0, om, 2)
+    e.fcycle(0, om, 2)
+    for l in range(o.levels):
+        assert_field_equal(o, e, "u", l)
+        assert_field_equal(o, e, "f", l)
+
+
 @pytest.mark.parametrize("ci", range(len(STRICT_CONFIGS)))
 def test_strict_bc_cycle_bit_exact(mgp_mod, gpu_ready, ci):
     cfg = cfg_of(STRICT_CONFIGS[ci], strict=True)
