@@ -69,6 +69,8 @@ typedef enum { MGP_CYCLE_RELAXATION = 0, MGP_CYCLE_V = 1, MGP_CYCLE_F = 2 } mgp_
 /* mgp_desc.flags */
 #define MGP_FLAG_STRICT_BC 1u /* honour the requested north/south/bottom kinds instead of the
                                  reference's resolution to Dirichlet (include/domain.h:140-145,191-192) */
+#define MGP_FLAG_REFINE_F32 16u /* iterative refinement, FP32 correction hierarchy (see mgp_solve) */
+#define MGP_FLAG_REFINE_F64 32u /* iterative refinement, FP64 correction hierarchy */
 #define MGP_FLAG_FUSED_SETUP 8u /* cycles form the residual inside the restriction kernel (one
                                    launch, r never stored) instead of residual + restriction */
 

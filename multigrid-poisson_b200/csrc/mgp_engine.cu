@@ -106,6 +106,11 @@ struct mgp_solver {
     std::map<std::tuple<int, int64_t, uint64_t, uint64_t>, GraphEntry> graphs;
     bool capturing = false;
     int64_t launches = 0;  // kernels launched on this solver (graph replays count their nodes)
+    // Iterative refinement: this solver holds level 0 in FP64 (u, f, r, boundary data) and
+    // `inner` the correction hierarchy (all levels, FP32 or FP64, zero boundary data).  The
+    // inner solver shares this solver's stream.
+    mgp_solver* inner = nullptr;
+    bool owns_stream = true;
 };
 
 namespace {
@@ -471,6 +476,96 @@ int read_norm(mgp_solver* s, double* out) {
     return MGP_OK;
 }
 
+// ---- iterative refinement ------------------------------------------------------------
+template <typename Ti>
+int refine_residual_t(mgp_solver* s, bool write_r) {
+    mgp_solver* in = s->inner;
+    LevelState& L = s->lv[0];
+    LevelState& I = in->lv[0];
+    RefineArgs<double, Ti> a;
+    a.G = L.G;
+    a.u = (const double*)u_ptr(s, 0);
+    a.f = (const double*)L.f;
+    a.r = (double*)L.r;
+    a.F = faces_of<double>(s, 0);
+    a.two_h = 2.0 * L.h;
+    a.hsq = L.h * L.h;
+    hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
+    a.sxi = I.G.sx;
+    a.syi = I.G.sy;
+    a.fi = (Ti*)I.f;
+    a.ui = (Ti*)u_ptr(in, 0);
+    a.norm = s->d_norm;
+    constexpr int V = VecT<double>::V;
+    const int plane = L.G.ny * ((L.G.nz + V - 1) / V);
+    const int bx = (plane + kThreads - 1) / kThreads;
+    const int target = sm_count(s->device) * 8;
+    int chunks = std::max(1, std::min((target + bx - 1) / bx, L.G.nx));
+    a.ichunk = (L.G.nx + chunks - 1) / chunks;
+    chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
+    CK(cudaMemsetAsync(s->d_norm, 0, sizeof(unsigned long long), s->stream));
+    if (write_r) k_refine_residual<double, Ti, true><<<dim3(bx, chunks), kThreads, 0, s->stream>>>(a);
+    else k_refine_residual<double, Ti, false><<<dim3(bx, chunks), kThreads, 0, s->stream>>>(a);
+    return check_launch(s);
+}
+
+template <typename Ti>
+int refine_update_t(mgp_solver* s) {
+    mgp_solver* in = s->inner;
+    LevelState& L = s->lv[0];
+    LevelState& I = in->lv[0];
+    const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
+    k_refine_update<double, Ti><<<grid_1d(s, n), kThreads, 0, s->stream>>>((double*)u_ptr(s, 0), L.G,
+                                                                            (const Ti*)u_ptr(in, 0), I.G.sx, I.G.sy);
+    return check_launch(s);
+}
+
+int refine_residual(mgp_solver* s, bool write_r) {
+    return s->inner->dtype == MGP_F32 ? refine_residual_t<float>(s, write_r) : refine_residual_t<double>(s, write_r);
+}
+
+// One refinement step, captured once per (cycle, nsmooth, omega, inner state): the
+// correction cycle on the inner hierarchy, u += e, and the new FP64 residual with its norm.
+int launch_refine_step(mgp_solver* s, int cycle, int64_t ns, double omega) {
+    mgp_solver* in = s->inner;
+    uint64_t ob;
+    memcpy(&ob, &omega, sizeof(ob));
+    auto key = std::make_tuple(100 + cycle, ns, ob, state_bits(in));
+    auto it = s->graphs.find(key);
+    if (it == s->graphs.end()) {
+        const uint64_t pre = state_bits(in);
+        const int64_t l0 = s->launches + in->launches;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        int st;
+        if (in->dtype == MGP_F32) {
+            st = cycle == MGP_CYCLE_V ? vcycle_t<float>(in, 0, omega, ns) : fcycle_t<float>(in, 0, omega, ns);
+            if (st == MGP_OK) st = refine_update_t<float>(s);
+        } else {
+            st = cycle == MGP_CYCLE_V ? vcycle_t<double>(in, 0, omega, ns) : fcycle_t<double>(in, 0, omega, ns);
+            if (st == MGP_OK) st = refine_update_t<double>(s);
+        }
+        if (st == MGP_OK) st = refine_residual(s, false);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        GraphEntry ge;
+        ge.post_state = state_bits(in);
+        ge.kernels = s->launches + in->launches - l0;
+        set_state_bits(in, pre);
+        if (st != MGP_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return st != MGP_OK ? st : fail(MGP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        }
+        cudaError_t ei = cudaGraphInstantiate(&ge.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return fail(MGP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+        it = s->graphs.emplace(key, ge).first;
+    }
+    CK(cudaGraphLaunch(it->second.exec, s->stream));
+    set_state_bits(in, it->second.post_state);
+    s->launches += it->second.kernels;
+    return MGP_OK;
+}
+
 int validate(const mgp_solver* s) { return s ? MGP_OK : fail(MGP_ERR_INVALID_ARG, "null solver"); }
 int validate_level(const mgp_solver* s, int l, bool need_coarser = false) {
     CKS(validate(s));
@@ -527,7 +622,8 @@ void release(mgp_solver* s) {
     }
     if (s->d_norm) cudaFree(s->d_norm);
     if (s->h_norm) cudaFreeHost(s->h_norm);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->inner) release(s->inner);
+    if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
 }
 
@@ -646,7 +742,7 @@ int mgp_plan_level(const mgp_desc* d, int l, mgp_level_info* out) {
     return MGP_OK;
 }
 
-int mgp_create(const mgp_desc* d, mgp_solver** out) {
+static int create_plain(const mgp_desc* d, mgp_solver** out) {
     if (!d || !out) return fail(MGP_ERR_INVALID_ARG, "null descriptor or out pointer");
     *out = nullptr;
     std::vector<mgp_level_info> plan(d->levels > 0 && d->levels <= 30 ? d->levels : 1);
@@ -728,6 +824,40 @@ int mgp_create(const mgp_desc* d, mgp_solver** out) {
                     cudaGetErrorString(e));
     }
     *out = s;
+    return MGP_OK;
+}
+
+int mgp_create(const mgp_desc* d, mgp_solver** out) {
+    if (!d || !out) return fail(MGP_ERR_INVALID_ARG, "null descriptor or out pointer");
+    *out = nullptr;
+    const uint32_t refine = d->flags & (MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64);
+    if (!refine) return create_plain(d, out);
+    if (refine == (MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64))
+        return fail(MGP_ERR_INVALID_ARG, "choose one of MGP_FLAG_REFINE_F32 / MGP_FLAG_REFINE_F64");
+    if (d->dtype != MGP_F64) return fail(MGP_ERR_INVALID_ARG, "a refinement solver keeps level 0 in FP64 (dtype F64)");
+    if (d->levels < 2) return fail(MGP_ERR_INVALID_ARG, "a refinement solver needs at least 2 levels");
+    // the correction hierarchy: every level, the requested inner precision
+    mgp_desc di = *d;
+    di.flags &= ~(MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64);
+    di.dtype = (refine & MGP_FLAG_REFINE_F32) ? MGP_F32 : MGP_F64;
+    // the outer level: FP64, level 0 only
+    mgp_desc dout = *d;
+    dout.flags &= ~(MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64);
+    dout.levels = 1;
+    mgp_solver* outer = nullptr;
+    CKS(create_plain(&dout, &outer));
+    mgp_solver* inner = nullptr;
+    int st = create_plain(&di, &inner);
+    if (st != MGP_OK) {
+        release(outer);
+        return st;
+    }
+    cudaStreamDestroy(inner->stream);
+    inner->stream = outer->stream;
+    inner->owns_stream = false;
+    outer->inner = inner;
+    outer->desc = *d;  // keeps the refine flag and the user's level count
+    *out = outer;
     return MGP_OK;
 }
 
@@ -904,9 +1034,64 @@ int mgp_get_stream(mgp_solver* s, void** stream) {
 }
 
 // ---- solve ----------------------------------------------------------------------------
+// Iterative refinement (MGP_FLAG_REFINE_F32 / _F64): r = f - A u in FP64 on level 0, one
+// correction cycle A e ~= r on the inner hierarchy (zero initial guess, zero boundary data),
+// u += e; repeated until ||r||inf / ||f||inf < tolerance, maxiter steps or maxtime.  The
+// correction equation uses the same discrete operator as the reference, so the converged u is
+// the reference discretisation's solution; unlike the reference's own cycle loop the
+// Neumann boundary data enter only through the FP64 residual, which removes the
+// reference's stagnation on Neumann problems.
+static int solve_refined(mgp_solver* s, int cycle, int64_t ns, double omega, double maxtime, uint32_t flags,
+                         mgp_stats* out) {
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
+    auto since = [&](clock::time_point a) { return std::chrono::duration<double>(clock::now() - a).count(); };
+    if (cycle != MGP_CYCLE_V && cycle != MGP_CYCLE_F)
+        return fail(MGP_ERR_INVALID_ARG, "refinement uses \"Vcycle\" or \"Fcycle\" corrections");
+    if (ns < 0) return fail(MGP_ERR_INVALID_ARG, "nsmooth must be >= 0");
+    DeviceGuard guard(s->device);
+    if (omega < 0) omega = s->desc.relaxation == MGP_JACOBI ? 6.0 / 7.0 : 8.0 / 9.0;
+    const int64_t launches_at_start = s->launches + s->inner->launches;
+    double fnorm = 0.0, rnorm = 0.0;
+    CK(cudaMemsetAsync(s->d_norm, 0, sizeof(unsigned long long), s->stream));
+    CKS(norm_t<double>(s, s->lv[0].f, 0, s->d_norm));
+    CKS(read_norm(s, &fnorm));
+    CKS(refine_residual(s, false));
+    CKS(read_norm(s, &rnorm));
+    double rel = rnorm / fnorm;
+    const double first = rel;
+    if (flags & MGP_SOLVE_VERBOSE)
+        std::cout << std::setw(4) << 0 << ": Initial residual: " << std::setw(8) << rel << std::endl;
+    int64_t it = 0;
+    while (it < s->desc.maxiter && !(rel < s->desc.tolerance)) {
+        if (since(t0) > maxtime) {
+            std::cout << "WARNING: Solver reached maximum wall time without converging!" << std::endl;
+            break;
+        }
+        CKS(launch_refine_step(s, cycle, ns, omega));
+        CKS(read_norm(s, &rnorm));
+        rel = rnorm / fnorm;
+        it++;
+        if (flags & MGP_SOLVE_VERBOSE)
+            std::cout << std::setw(4) << it << ": Relative residual: " << std::setw(8) << rel << std::endl;
+    }
+    CKS(refine_residual(s, true));  // the user-visible FP64 residual of the returned u
+    CK(cudaStreamSynchronize(s->stream));
+    if (out) {
+        out->rel_res = rel;
+        out->iterations = (double)it;
+        out->seconds = since(t0);
+        out->cycles_run = it;
+        out->first_rel_res = first;
+        out->kernel_launches = s->launches + s->inner->launches - launches_at_start;
+    }
+    return MGP_OK;
+}
+
 int mgp_solve(mgp_solver* s, int cycle, int64_t nsmooth, double omega, const char* ofile, double maxtime,
               uint32_t flags, mgp_stats* out) {
     CKS(validate(s));
+    if (s->inner) return solve_refined(s, cycle, nsmooth, omega, maxtime, flags, out);
     using clock = std::chrono::steady_clock;
     const auto t0 = clock::now();
     auto since = [&](clock::time_point a) { return std::chrono::duration<double>(clock::now() - a).count(); };

@@ -731,6 +731,154 @@ __global__ void __launch_bounds__(256) k_norm(const T* __restrict__ a, Geom G, u
     block_max_to(mx, out);
 }
 
+// ------------------------------------------------------------------------------------
+// Iterative refinement.  The outer level keeps u, f and the boundary data in FP64; a
+// correction e with A e = r and homogeneous boundary data (Dirichlet 0, Neumann ghost =
+// mirror) is solved on an inner hierarchy of type Ti, then u += e.
+//
+// k_refine_residual: r = f - A u (the reference's residual with its ghost rule) over the
+// relaxation bounds; writes (Ti) r into the inner right-hand side, zeroes the inner initial
+// guess, reduces max |r|, and with WRITE_R also stores r (the user-visible residual).
+template <typename T, typename Ti>
+struct RefineArgs {
+    Geom G;                 // outer level 0
+    const T* u;
+    const T* f;
+    T* r;
+    Faces<T> F;
+    T two_h, hsq, inv_hsq;
+    int hsq_pow2;
+    int ichunk;
+    long long sxi, syi;     // inner level-0 strides
+    Ti* fi;                 // inner right-hand side
+    Ti* ui;                 // inner initial guess (zeroed) / correction (read by the update)
+    unsigned long long* norm;
+};
+
+template <typename T, typename Ti, bool WRITE_R>
+__global__ void __launch_bounds__(256) k_refine_residual(RefineArgs<T, Ti> a) {
+    constexpr int V = VecT<T>::V;
+    const Geom& G = a.G;
+    const int nv = (G.nz + V - 1) / V;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ia = blockIdx.y * a.ichunk;
+    const int ib = min(G.nx, ia + a.ichunk);
+    unsigned long long mx = 0ull;
+    if (t < G.ny * nv) {
+        const int j = t / nv;
+        const int kb = (t - j * nv) * V;
+        const long long bjk = (long long)j * G.sy + kb;
+        const long long bjki = (long long)j * a.syi + kb;
+        const bool jin = j >= G.y0 && j < G.y1;
+        unsigned ins = 0u, inr = 0u;
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const int k = kb + e;
+            if (k < G.nz) ins |= 1u << e;
+            if (jin && k >= G.z0 && k < G.z1) inr |= 1u << e;
+        }
+        const int i0 = max(ia, G.x0);
+        const int i1 = inr ? min(ib, G.x1) : i0;
+        if (i0 < i1) {
+            const T two_h = a.two_h, m2h = -a.two_h;
+            T vm[V], vc[V], vp[V], vpp[V], fc[V], fn[V];
+            ldv(vc, a.u + (long long)i0 * G.sx + bjk);
+            if (i0 > 0) {
+                ldv(vm, a.u + (long long)(i0 - 1) * G.sx + bjk);
+            } else {
+                T v1[V];
+                ldv(v1, a.u + G.sx + bjk);
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    vm[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_WEST] + (long long)j * G.nz + kb + e) + v1[e] : T(0);
+            }
+            if (i0 + 1 < G.nx) ldv(vp, a.u + (long long)(i0 + 1) * G.sx + bjk);
+            ldv(fc, a.f + (long long)i0 * G.sx + bjk);
+            for (int i = i0; i < i1; i++) {
+                const long long p = (long long)i * G.sx + bjk;
+                if (i + 1 < i1) {
+                    if (i + 2 < G.nx) ldv(vpp, a.u + p + 2 * G.sx);
+                    ldv(fn, a.f + p + G.sx);
+                }
+                if (i + 1 == G.nx) {
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + kb + e) + vm[e]
+                                                  : T(0);
+                }
+                T ym[V], yp[V];
+                if (j > 0) {
+                    ldv(ym, a.u + p - G.sy);
+                } else {
+                    T w[V];
+                    ldv(w, a.u + p + G.sy);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        ym[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_SOUTH] + (long long)i * G.nz + kb + e) + w[e] : T(0);
+                }
+                if (j < G.ny - 1) {
+                    ldv(yp, a.u + p + G.sy);
+                } else {
+                    T w[V];
+                    ldv(w, a.u + p - G.sy);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        yp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_NORTH] + (long long)i * G.nz + kb + e) + w[e]
+                                                  : T(0);
+                }
+                const T left = kb > 0 ? ldg(a.u + p - 1) : T(0);
+                const T right = kb + V < G.nz ? ldg(a.u + p + V) : T(0);
+                T rv[V];
+#pragma unroll
+                for (int e = 0; e < V; e++) {
+                    rv[e] = T(0);
+                    if (!((inr >> e) & 1u)) continue;
+                    const int k = kb + e;
+                    const T below = e > 0 ? vc[e - 1] : left;
+                    const T above = e < V - 1 ? vc[e + 1] : right;
+                    const T zm = k > 0 ? below : m2h * ldg(a.F.g[F_BOTTOM] + (long long)i * G.ny + j) + vc[1];
+                    const T zp = k < G.nz - 1 ? above : two_h * ldg(a.F.g[F_TOP] + (long long)i * G.ny + j) + below;
+                    const T sum = vm[e] + vp[e] + ym[e] + yp[e] + zm + zp;
+                    rv[e] = residual_pt(fc[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
+                    mx = max(mx, abs_bits(rv[e]));
+                }
+                const long long q = (long long)i * a.sxi + bjki;
+#pragma unroll
+                for (int e = 0; e < V; e++) {
+                    if (!((inr >> e) & 1u)) continue;
+                    a.fi[q + e] = (Ti)rv[e];
+                    a.ui[q + e] = Ti(0);
+                    if (WRITE_R) a.r[p + e] = rv[e];
+                }
+#pragma unroll
+                for (int e = 0; e < V; e++) {
+                    vm[e] = vc[e];
+                    vc[e] = vp[e];
+                    vp[e] = vpp[e];
+                    fc[e] = fn[e];
+                }
+            }
+        }
+    }
+    block_max_to(mx, a.norm);
+}
+
+// u += (T) e over the relaxation bounds (e: the inner level-0 solution).
+template <typename T, typename Ti>
+__global__ void __launch_bounds__(256) k_refine_update(T* u, Geom G, const Ti* __restrict__ e, long long sxi,
+                                                       long long syi) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        if (i < G.x0 || i >= G.x1 || j < G.y0 || j >= G.y1 || k < G.z0 || k >= G.z1) continue;
+        const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
+        u[p] = u[p] + (T)ldg(e + (long long)i * sxi + (long long)j * syi + k);
+    }
+}
+
 // Dirichlet::write_to (include/dirichlet.h:50-93): one face into its boundary plane.
 template <typename T>
 __global__ void __launch_bounds__(256) k_write_face(T* u, Geom G, const T* __restrict__ g, int fc) {

@@ -37,6 +37,8 @@ FIELDS = ("u", "uprev", "f", "r")
 CYCLE_RELAXATION, CYCLE_V, CYCLE_F = 0, 1, 2
 FLAG_STRICT_BC = 1
 FLAG_FUSED_SETUP = 8
+FLAG_REFINE_F32 = 16
+FLAG_REFINE_F64 = 32
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,
@@ -195,7 +197,8 @@ class Solver:
         self.np_dtype = _np_dtype(dtype)
         self.levels = levels
         self.level = []
-        for l in range(levels):
+        # a refinement solver exposes its FP64 level 0 only (the correction hierarchy is internal)
+        for l in range(L.mgp_num_levels(self._h)):
             li = LevelInfo()
             _check(L.mgp_level_info_get(self._h, l, ctypes.byref(li)))
             self.level.append(Level(tuple(li.shape), dict(zip(("east", "west", "north", "south", "top", "bottom"),
