@@ -194,7 +194,8 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
     dim3 grid(bx, chunks);
-    k_stencil<T, OP><<<grid, kThreads, 0, s->stream>>>(a);
+    if (OP == OP_RESIDUAL && norm) k_stencil<T, OP, true><<<grid, kThreads, 0, s->stream>>>(a);
+    else k_stencil<T, OP, false><<<grid, kThreads, 0, s->stream>>>(a);
     return check_launch(s);
 }
 
@@ -276,8 +277,8 @@ int prolong_t(mgp_solver* s, int l) {
     LevelState& F = s->lv[l];
     LevelState& C = s->lv[l + 1];
     constexpr int V = VecT<T>::V;
-    const int rows = F.G.ny * ((F.G.nz + V - 1) / V);
-    dim3 grid((rows + kThreads - 1) / kThreads, F.G.nx);
+    const int rows = C.G.ny * ((F.G.nz + V - 1) / V);  // one thread per coarse (j) row x fine k-vector
+    dim3 grid((rows + kThreads - 1) / kThreads, C.G.nx);
     k_prolong<T, ADD><<<grid, kThreads, 0, s->stream>>>((const T*)u_ptr(s, l + 1), C.G, (T*)u_ptr(s, l), (T*)F.r, F.G);
     return check_launch(s);
 }

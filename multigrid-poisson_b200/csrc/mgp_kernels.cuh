@@ -157,12 +157,37 @@ __device__ __forceinline__ void stv(float* p, const float (&d)[4]) {
     *reinterpret_cast<float4*>(p) = make_float4(d[0], d[1], d[2], d[3]);
 }
 
+// Asynchronous 16-byte global->shared copies (cp.async, cached in L1 so that neighbouring
+// threads' in-plane reads of the same plane still hit L1).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void lds_v(T (&d)[VecT<T>::V], const T* p) {
+#pragma unroll
+    for (int e = 0; e < VecT<T>::V; e++) d[e] = p[e];
+}
+
+constexpr int kStages = 4;  // planes of u and f in flight per thread
+
 // One thread owns a V-vector of k points of one (j) row and marches i over a chunk of
-// planes; the next plane of u and f are prefetched one step ahead.  For small levels the
-// chunk is a single plane, which turns the march into one point-vector per thread.
-template <typename T, int OP>
+// planes with u(i-1), u(i), u(i+1) in registers.  The next kStages planes of u and f are
+// staged by cp.async into the thread's own shared-memory slots, so each thread keeps
+// 2*kStages*16 bytes in flight without a block barrier.  For small levels the chunk is a
+// single plane (one point-vector per thread).  NORM adds the max-norm of the residual
+// over the whole shape.
+template <typename T, int OP, bool NORM>
 __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
     constexpr int V = VecT<T>::V;
+    __shared__ __align__(16) T stage_u[kStages][256 * V];
+    __shared__ __align__(16) T stage_f[kStages][256 * V];
     const Geom& G = a.G;
     const int nv = (G.nz + V - 1) / V;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,7 +209,7 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
         const unsigned full = (1u << V) - 1u;
         const int i0 = max(ia, G.x0);
         const int i1 = inr ? min(ib, G.x1) : i0;
-        if (OP == OP_RESIDUAL && a.norm) {
+        if (NORM) {
             // r outside the bounds keeps its value and still counts in the norm
             // (infinity_norm runs over the whole shape, devicearray.h:221-237).
             for (int i = ia; i < ib; i++) {
@@ -203,7 +228,20 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
             const T* f = a.f;
             const T two_h = a.two_h;
             const T m2h = -two_h;
-            T vm[V], vc[V], vp[V], vpp[V], fc[V], fn[V], vmo[V];
+            T* su = &stage_u[0][threadIdx.x * V];
+            T* sf = &stage_f[0][threadIdx.x * V];
+            constexpr int SS = 256 * V;  // stage stride
+            // stage s holds u(i0+s+1) and f(i0+s)
+#pragma unroll
+            for (int st = 0; st < kStages; st++) {
+                const int p = i0 + st;
+                if (p < i1) {
+                    if (p + 1 < G.nx) cp_async16(su + st * SS, src + (long long)(p + 1) * G.sx + bjk);
+                    cp_async16(sf + st * SS, f + (long long)p * G.sx + bjk);
+                }
+                cp_async_commit();
+            }
+            T vm[V], vc[V], vp[V], fc[V], vmo[V];
             ldv(vc, src + (long long)i0 * G.sx + bjk);
             if (i0 > 0) {
                 ldv(vm, src + (long long)(i0 - 1) * G.sx + bjk);
@@ -216,19 +254,26 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
             }
 #pragma unroll
             for (int e = 0; e < V; e++) vmo[e] = vm[e];
-            if (i0 + 1 < G.nx) ldv(vp, src + (long long)(i0 + 1) * G.sx + bjk);
-            ldv(fc, f + (long long)i0 * G.sx + bjk);
             for (int i = i0; i < i1; i++) {
                 const long long p = (long long)i * G.sx + bjk;
-                if (i + 1 < i1) {
-                    if (i + 2 < G.nx) ldv(vpp, src + p + 2 * G.sx);
-                    ldv(fn, f + p + G.sx);
-                }
-                if (i + 1 == G.nx) {  // east ghost  2h*gE + u(nx-2), from before this sweep
+                const int slot = (i - i0) % kStages;
+                cp_async_wait<kStages - 1>();
+                if (i + 1 < G.nx) {
+                    lds_v(vp, su + slot * SS);
+                } else {  // east ghost  2h*gE + u(nx-2), from before this sweep
 #pragma unroll
                     for (int e = 0; e < V; e++)
                         vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + kb + e) + vmo[e]
                                                   : T(0);
+                }
+                lds_v(fc, sf + slot * SS);
+                {  // refill this slot with plane i+kStages
+                    const int q = i + kStages;
+                    if (q < i1) {
+                        if (q + 1 < G.nx) cp_async16(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
+                        cp_async16(sf + slot * SS, f + (long long)q * G.sx + bjk);
+                    }
+                    cp_async_commit();
                 }
                 unsigned act = inr;
                 if (OP == OP_GS || OP == OP_GS_COLUMN) {
@@ -279,7 +324,7 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
                         if (OP == OP_RESIDUAL) {
                             const T r = residual_pt(fc[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
                             cur[e] = r;
-                            mx = max(mx, abs_bits(r));
+                            if (NORM) mx = max(mx, abs_bits(r));
                         } else {
                             // jacobi.h:59-61 / gaussseidel.h:43-45:
                             //   u = one_omega*v + omega_sixth*(sum - hsq*f)
@@ -305,13 +350,12 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
                     // residual keep marching over the source iterate
                     vm[e] = (OP == OP_GS || OP == OP_GS_COLUMN) ? cur[e] : vc[e];
                     vc[e] = vp[e];
-                    vp[e] = vpp[e];
-                    fc[e] = fn[e];
                 }
             }
+            cp_async_wait<0>();
         }
     }
-    if (OP == OP_RESIDUAL && a.norm) block_max_to(mx, a.norm);
+    if (NORM) block_max_to(mx, a.norm);
 }
 
 // ------------------------------------------------------------------------------------
@@ -634,70 +678,88 @@ __device__ __forceinline__ T half_sum(T a, T b) {
     return (T)(0.5 * (a + b));
 }
 
+// One thread: fine rows (2ic..2ic+1, 2jc..2jc+1) at one k-vector, from the coarse values
+// (ic..ic+1, jc..jc+1, kb/2..kb/2+V/2) -- each coarse value is loaded once per thread.
 template <typename T, bool ADD>
 __global__ void __launch_bounds__(256) k_prolong(const T* __restrict__ uc, Geom Gc, T* u, T* r, Geom Gf) {
-    // one thread: a V-vector of fine k points of row (i = blockIdx.y, j)
     constexpr int V = VecT<T>::V;
+    constexpr int NQ = V / 2 + 1;
     const int nv = (Gf.nz + V - 1) / V;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= Gf.ny * nv) return;
-    const int i = blockIdx.y;
-    const int j = t / nv;
-    const int kb = (t - j * nv) * V;  // even
-    const int ic = i >> 1, jc = j >> 1;
-    auto C = [&](int x, int y, int z) -> T { return ldg(uc + x * Gc.sx + y * Gc.sy + z); };
-    auto X = [&](int y, int z) -> T {  // value at (i, 2y, 2z) after the x pass
-        T v = C(ic, y, z);
-        if (i & 1) v = half_sum(v, C(ic + 1, y, z));
-        return v;
-    };
-    auto Y = [&](int z) -> T {  // value at (i, j, 2z) after the y pass
-        if (j & 1) return half_sum(X(jc, z), X(jc + 1, z));
-        return X(jc, z);
-    };
-    constexpr int NQ = V / 2 + 1;
-    T yv[NQ];
+    if (t >= Gc.ny * nv) return;
+    const int ic = blockIdx.y;
+    const int jc = t / nv;
+    const int kb = (t - jc * nv) * V;  // even
+    const bool i_odd_ok = 2 * ic + 1 < Gf.nx, j_odd_ok = 2 * jc + 1 < Gf.ny;
+    // coarse values c[a][b][q] = C(ic+a, jc+b, kb/2+q)
+    T c[2][2][NQ];
 #pragma unroll
-    for (int q = 0; q < NQ; q++) {
-        const int z = (kb >> 1) + q;
-        yv[q] = z < Gc.nz ? Y(z) : T(0);
-    }
-    T ev[V];
-    unsigned ins = 0u, inside = 0u;
-    const bool ijin = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1;
+    for (int a2 = 0; a2 < 2; a2++)
 #pragma unroll
-    for (int e = 0; e < V; e++) {
-        const int k = kb + e;
-        // z pass: odd k averages the two neighbouring even-k values
-        ev[e] = (e & 1) ? half_sum(yv[e >> 1], yv[(e >> 1) + 1]) : yv[e >> 1];
-        if (k < Gf.nz) ins |= 1u << e;
-        if (ijin && k >= Gf.z0 && k < Gf.z1) inside |= 1u << e;
-    }
-    const long long p = (long long)i * Gf.sx + (long long)j * Gf.sy + kb;
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const int x = ic + a2, y = jc + b, z = (kb >> 1) + q;
+                c[a2][b][q] = (x < Gc.nx && y < Gc.ny && z < Gc.nz) ? ldg(uc + x * Gc.sx + y * Gc.sy + z) : T(0);
+            }
+    unsigned ins = 0u;
+#pragma unroll
+    for (int e = 0; e < V; e++)
+        if (kb + e < Gf.nz) ins |= 1u << e;
     const unsigned full = (1u << V) - 1u;
-    if (ADD) {
-        if (ins == full) {
-            T uv[V];
-            ldv_rw(uv, u + p);
 #pragma unroll
-            for (int e = 0; e < V; e++) uv[e] = uv[e] + ev[e];
-            stv(u + p, uv);
-        } else {
+    for (int ip = 0; ip < 2; ip++) {
+        if (ip && !i_odd_ok) continue;
+        const int i = 2 * ic + ip;
+#pragma unroll
+        for (int jp = 0; jp < 2; jp++) {
+            if (jp && !j_odd_ok) continue;
+            const int j = 2 * jc + jp;
+            // x pass (odd i: midpoint of the two coarse planes), then y pass, per coarse z
+            T yv[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                T x0 = c[0][0][q], x1 = c[0][1][q];
+                if (ip) {
+                    x0 = half_sum(x0, c[1][0][q]);
+                    x1 = half_sum(x1, c[1][1][q]);
+                }
+                yv[q] = jp ? half_sum(x0, x1) : x0;
+            }
+            T ev[V];
+#pragma unroll
+            for (int e = 0; e < V; e++) ev[e] = (e & 1) ? half_sum(yv[e >> 1], yv[(e >> 1) + 1]) : yv[e >> 1];
+            const long long p = (long long)i * Gf.sx + (long long)j * Gf.sy + kb;
+            const bool ijin = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1;
+            unsigned inside = 0u;
 #pragma unroll
             for (int e = 0; e < V; e++)
-                if ((ins >> e) & 1u) u[p + e] = u[p + e] + ev[e];
-        }
-        const unsigned rm = ins & ~inside;
+                if (ijin && kb + e >= Gf.z0 && kb + e < Gf.z1) inside |= 1u << e;
+            if (ADD) {
+                if (ins == full) {
+                    T uv[V];
+                    ldv_rw(uv, u + p);
 #pragma unroll
-        for (int e = 0; e < V; e++)
-            if ((rm >> e) & 1u) r[p + e] = ev[e];
-    } else {
-        if (ins == full) {
-            stv(r + p, ev);
-        } else {
+                    for (int e = 0; e < V; e++) uv[e] = uv[e] + ev[e];
+                    stv(u + p, uv);
+                } else {
 #pragma unroll
-            for (int e = 0; e < V; e++)
-                if ((ins >> e) & 1u) r[p + e] = ev[e];
+                    for (int e = 0; e < V; e++)
+                        if ((ins >> e) & 1u) u[p + e] = u[p + e] + ev[e];
+                }
+                const unsigned rm = ins & ~inside;
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    if ((rm >> e) & 1u) r[p + e] = ev[e];
+            } else {
+                if (ins == full) {
+                    stv(r + p, ev);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if ((ins >> e) & 1u) r[p + e] = ev[e];
+                }
+            }
         }
     }
 }
