@@ -203,6 +203,56 @@ int mgp_synchronize(mgp_solver* s);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int mgp_get_stream(mgp_solver* s, void** stream);
 
+/* ---- batches: many independent problems solved together ----------------------------
+ * A batch holds refinement solvers (FP64 level 0, correction hierarchy in inner_dtype) of any
+ * sizes and level counts.  One mgp_batch_step() is one refinement step (correction cycle,
+ * u += e, FP64 residual) for every active problem; each level operation is ONE persistent
+ * kernel launch over a (problem, tile) work list covering every problem that takes part in
+ * it (problems are aligned by depth below their finest level).  No counterpart in the
+ * reference, which solves one problem per PoissonSolver. */
+typedef struct mgp_batch_desc {
+    int32_t restriction;   /* mgp_restriction, shared by all problems */
+    int32_t relaxation;    /* mgp_relaxation */
+    int32_t inner_dtype;   /* MGP_F32 (mixed precision) or MGP_F64 */
+    int32_t cycle;         /* MGP_CYCLE_F or MGP_CYCLE_V */
+    int64_t nsmooth;
+    double omega;          /* < 0: the relaxation's default */
+    int64_t max_problems;  /* capacity (problems resident at once) */
+    int32_t device;
+    uint32_t flags;
+} mgp_batch_desc;
+typedef struct mgp_batch mgp_batch;
+int mgp_batch_create(const mgp_batch_desc* desc, mgp_batch** out);
+int mgp_batch_destroy(mgp_batch* b);
+/* Device bytes one problem takes in a batch (for admission by free device memory). */
+int mgp_batch_problem_bytes(const mgp_batch_desc* bdesc, const mgp_desc* problem, int64_t* bytes);
+/* Allocates a problem (dims, levels, h, bc, origin of `problem`; the batch's operators and
+ * precision).  Load its data through mgp_batch_problem() + mgp_upload_* + mgp_write_bc. */
+int mgp_batch_add(mgp_batch* b, const mgp_desc* problem, int* id);
+int mgp_batch_problem(mgp_batch* b, int id, mgp_solver** s);
+int mgp_batch_remove(mgp_batch* b, int id);
+int mgp_batch_set_active(mgp_batch* b, int id, int active);
+/* One refinement step for every active problem (problems added since the last step first get
+ * their initial residual).  n_active: problems stepped. */
+int mgp_batch_step(mgp_batch* b, int* n_active);
+/* rel_res / iterations / first_rel_res of one problem. */
+int mgp_batch_status(mgp_batch* b, int id, mgp_stats* out);
+/* Steps until every active problem has ||r||inf/||f||inf < tol (each problem stops when it
+ * gets there) or maxiter steps; then stores every problem's FP64 residual. */
+int mgp_batch_solve(mgp_batch* b, double tol, int64_t maxiter, int64_t* steps);
+/* Kernel launches of one step for the current active set. */
+int mgp_batch_kernel_launches(const mgp_batch* b, int64_t* per_step);
+
+/* Free and total device memory (cudaMemGetInfo) of `device`, for admission control. */
+int mgp_mem_info(int device, size_t* free_bytes, size_t* total_bytes);
+/* Device-side right-hand side: level-0 f of an FP64 (or refinement) solver set to
+ *   f(x,y,z) = sum_m amp[m] sin(kx[m] pi x/L[0]) sin(ky[m] pi y/L[1]) sin(kz[m] pi z/L[2])
+ * at every shape point, (x,y,z) = (i,j,k)*h measured from the origin (n_modes <= 64).  The
+ * host-side alternative is to sample f and mgp_upload_field it; this skips the host and
+ * the PCIe copy.  No counterpart in the reference (its init() samples ffun on the host). */
+int mgp_fill_sine_modes(mgp_solver* s, int n_modes, const double* amp, const double* kx, const double* ky,
+                        const double* kz, const double L[3]);
+
 /* Page-locked host memory for field buffers (faster uploads/downloads). */
 int mgp_host_alloc(void** p, size_t bytes);
 int mgp_host_free(void* p);

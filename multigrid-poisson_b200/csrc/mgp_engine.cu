@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <iomanip>
 #include <iostream>
 #include <map>
@@ -152,6 +153,38 @@ int check_launch(mgp_solver* s) {
     return MGP_OK;
 }
 
+// Blocks of `kernel` resident per SM (256 threads, static shared memory only).
+template <typename K>
+int resident_blocks(K kernel) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
+
+// Planes per block of a marching kernel: bx blocks cover a plane, `chunks` split the march.
+// Small levels march one plane per thread.  Large levels choose the chunk count whose whole
+// grid fills the resident block slots best (a few blocks in an extra wave would run alone),
+// counting the two planes each chunk re-reads at its start.
+int march_chunks(int bx, int nx, int cap) {
+    if ((long long)bx * nx <= cap) return nx;
+    int best = 1;
+    double best_eff = -1.0;
+    for (int waves = 1; waves <= 8; waves++) {
+        int c = (int)std::min<long long>(nx, std::max(1ll, (long long)waves * cap / bx));
+        const long long blocks = (long long)bx * c;
+        const long long w = (blocks + cap - 1) / cap;
+        const int ichunk = (nx + c - 1) / c;
+        const double fill = (double)blocks / (double)(w * cap);
+        const double reread = 1.0 / (1.0 + 2.0 / (3.0 * ichunk));
+        const double eff = fill * reread;
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = c;
+        }
+    }
+    return best;
+}
+
 // x/hsq equals x*(1/hsq) bit for bit when hsq is a power of two (scaling by 2^k is exact);
 // the kernels then multiply instead of dividing.
 template <typename T>
@@ -187,9 +220,10 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     const int bx = (plane + kThreads - 1) / kThreads;
     int chunks = 1;
     if (OP != OP_GS_COLUMN) {
-        // enough blocks for ~2 waves; small levels get one plane per thread
-        const int target = sm_count(s->device) * 8;
-        chunks = std::max(1, std::min((target + bx - 1) / bx, L.G.nx));
+        const bool nrm = OP == OP_RESIDUAL && norm;
+        const int cap = sm_count(s->device) *
+                        (nrm ? resident_blocks(k_stencil<T, OP, true>) : resident_blocks(k_stencil<T, OP, false>));
+        chunks = march_chunks(bx, L.G.nx, cap);
     }
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
@@ -240,16 +274,25 @@ View face_view(const int64_t* fs) {
 }
 
 template <typename T>
-int restrict_t(mgp_solver* s, int l, bool zero_coarse_u) {
+RestrictArgs<T> restrict_args(mgp_solver* s, int l, bool zero_coarse_u, long long* npts) {
     LevelState& F = s->lv[l];
     LevelState& C = s->lv[l + 1];
-    View vi = level_view(F), vo = level_view(C);
-    const long long n = (long long)C.G.nx * C.G.ny * C.G.nz;
-    T* zu = zero_coarse_u ? (T*)u_ptr(s, l + 1) : nullptr;
-    if (s->desc.restriction == MGP_FULLWEIGHTING)
-        k_restrict<T, true><<<grid_1d(s, n), kThreads, 0, s->stream>>>((const T*)F.r, vi, (T*)C.f, vo, zu);
-    else
-        k_restrict<T, false><<<grid_1d(s, n), kThreads, 0, s->stream>>>((const T*)F.r, vi, (T*)C.f, vo, zu);
+    RestrictArgs<T> a;
+    a.in = (const T*)F.r;
+    a.vi = level_view(F);
+    a.out = (T*)C.f;
+    a.vo = level_view(C);
+    a.zero_u = zero_coarse_u ? (T*)u_ptr(s, l + 1) : nullptr;
+    a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
+    *npts = (long long)C.G.nx * C.G.ny * C.G.nz;
+    return a;
+}
+
+template <typename T>
+int restrict_t(mgp_solver* s, int l, bool zero_coarse_u) {
+    long long n = 0;
+    RestrictArgs<T> a = restrict_args<T>(s, l, zero_coarse_u, &n);
+    k_restrict<T><<<grid_1d(s, n), kThreads, 0, s->stream>>>(a);
     return check_launch(s);
 }
 
@@ -279,7 +322,8 @@ int prolong_t(mgp_solver* s, int l) {
     constexpr int V = VecT<T>::V;
     const int rows = C.G.ny * ((F.G.nz + V - 1) / V);  // one thread per coarse (j) row x fine k-vector
     dim3 grid((rows + kThreads - 1) / kThreads, C.G.nx);
-    k_prolong<T, ADD><<<grid, kThreads, 0, s->stream>>>((const T*)u_ptr(s, l + 1), C.G, (T*)u_ptr(s, l), (T*)F.r, F.G);
+    ProlongArgs<T> a{(const T*)u_ptr(s, l + 1), C.G, (T*)u_ptr(s, l), (T*)F.r, F.G};
+    k_prolong<T, ADD><<<grid, kThreads, 0, s->stream>>>(a);
     return check_launch(s);
 }
 
@@ -516,8 +560,8 @@ int refine_update_t(mgp_solver* s) {
     LevelState& L = s->lv[0];
     LevelState& I = in->lv[0];
     const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
-    k_refine_update<double, Ti><<<grid_1d(s, n), kThreads, 0, s->stream>>>((double*)u_ptr(s, 0), L.G,
-                                                                            (const Ti*)u_ptr(in, 0), I.G.sx, I.G.sy);
+    UpdateArgs<double, Ti> a{(double*)u_ptr(s, 0), L.G, (const Ti*)u_ptr(in, 0), I.G.sx, I.G.sy};
+    k_refine_update<double, Ti><<<grid_1d(s, n), kThreads, 0, s->stream>>>(a);
     return check_launch(s);
 }
 
@@ -1170,6 +1214,48 @@ int mgp_solve(mgp_solver* s, int cycle, int64_t nsmooth, double omega, const cha
     return MGP_OK;
 }
 
+int mgp_mem_info(int device, size_t* free_bytes, size_t* total_bytes) {
+    if (!free_bytes || !total_bytes) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(MGP_ERR_NO_DEVICE, "device %d not present", device);
+    DeviceGuard guard(device);
+    CK(cudaMemGetInfo(free_bytes, total_bytes));
+    return MGP_OK;
+}
+
+int mgp_fill_sine_modes(mgp_solver* s, int n_modes, const double* amp, const double* kx, const double* ky,
+                        const double* kz, const double L[3]) {
+    CKS(validate(s));
+    if (s->dtype != MGP_F64) return fail(MGP_ERR_INVALID_ARG, "the sine-mode fill writes an FP64 right-hand side");
+    if (n_modes < 0 || n_modes > 64 || (n_modes && (!amp || !kx || !ky || !kz)) || !L)
+        return fail(MGP_ERR_INVALID_ARG, "need 0..64 modes and L[3]");
+    const double pi = 3.14159265358979323846;
+    SineModes m{};
+    m.n = n_modes;
+    for (int i = 0; i < n_modes; i++) {
+        m.amp[i] = amp[i];
+        m.wx[i] = kx[i] * pi / L[0];
+        m.wy[i] = ky[i] * pi / L[1];
+        m.wz[i] = kz[i] * pi / L[2];
+    }
+    DeviceGuard guard(s->device);
+    SineModes* dm = nullptr;
+    CK(cudaMallocAsync((void**)&dm, sizeof(SineModes), s->stream));
+    cudaError_t e = cudaMemcpyAsync(dm, &m, sizeof(SineModes), cudaMemcpyHostToDevice, s->stream);
+    LevelState& L0 = s->lv[0];
+    const long long n = (long long)L0.G.nx * L0.G.ny * L0.G.nz;
+    if (e == cudaSuccess) {
+        k_fill_sine<<<grid_1d(s, n), kThreads, 0, s->stream>>>((double*)L0.f, L0.G, L0.h, dm);
+        e = cudaGetLastError();
+        s->launches++;
+    }
+    cudaFreeAsync(dm, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(MGP_ERR_CUDA, "sine-mode fill: %s", cudaGetErrorString(e));
+    return MGP_OK;
+}
+
 int mgp_host_alloc(void** p, size_t bytes) {
     if (!p) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
     CK(cudaMallocHost(p, bytes));
@@ -1181,3 +1267,5 @@ int mgp_host_free(void* p) {
 }
 
 }  // extern "C"
+
+#include "mgp_batch.cuh"

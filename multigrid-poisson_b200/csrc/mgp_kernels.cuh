@@ -184,14 +184,14 @@ constexpr int kStages = 4;  // planes of u and f in flight per thread
 // single plane (one point-vector per thread).  NORM adds the max-norm of the residual
 // over the whole shape.
 template <typename T, int OP, bool NORM>
-__global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
+__device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int bx, const int by) {
     constexpr int V = VecT<T>::V;
     __shared__ __align__(16) T stage_u[kStages][256 * V];
     __shared__ __align__(16) T stage_f[kStages][256 * V];
     const Geom& G = a.G;
     const int nv = (G.nz + V - 1) / V;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ia = blockIdx.y * a.ichunk;
+    const int t = bx * 256 + threadIdx.x;
+    const int ia = by * a.ichunk;
     const int ib = min(G.nx, ia + a.ichunk);
     unsigned long long mx = 0ull;
     if (t < G.ny * nv) {
@@ -358,6 +358,11 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
     if (NORM) block_max_to(mx, a.norm);
 }
 
+template <typename T, int OP, bool NORM>
+__global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
+    stencil_tile<T, OP, NORM>(a, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------------------------------
 // Restriction r_l -> f_{l+1} over the coarse shape, with u_{l+1} = 0 fused in
 // (include/vcycle.h:43-50).  Works on any pair of (shape, strides) views, so the same code
@@ -391,22 +396,38 @@ __device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j,
     return (T)((double)tmp / 64.0);
 }
 
-template <typename T, bool FW>
-__global__ void __launch_bounds__(256) k_restrict(const T* __restrict__ in, View vi, T* __restrict__ out, View vo,
-                                                  T* __restrict__ zero_u) {
+template <typename T>
+struct RestrictArgs {
+    const T* in;
+    View vi;
+    T* out;
+    View vo;
+    T* zero_u;  // coarse u to zero alongside (nullptr: none)
+    int fw;
+};
+
+// coarse points bx*256 + tid, bx*256 + tid + gx*256, ...
+template <typename T>
+__device__ __forceinline__ void restrict_tile(const RestrictArgs<T>& a, const int bx, const int gx) {
+    const View vo = a.vo;
     const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = bx * 256ll + threadIdx.x; t < n; t += gx * 256ll) {
         const int k = (int)(t % vo.n[2]);
         const long long q = t / vo.n[2];
         const int j = (int)(q % vo.n[1]);
         const int i = (int)(q / vo.n[1]);
         const long long o = i * vo.s0 + j * vo.s1 + k;
         T v;
-        if (FW) v = fw_point(in, vi, i, j, k);
-        else v = ldg(in + (2 * i) * vi.s0 + (2 * j) * vi.s1 + 2 * k);  // injection.h:63
-        out[o] = v;
-        if (zero_u) zero_u[o] = T(0);
+        if (a.fw) v = fw_point(a.in, a.vi, i, j, k);
+        else v = ldg(a.in + (2 * i) * a.vi.s0 + (2 * j) * a.vi.s1 + 2 * k);  // injection.h:63
+        a.out[o] = v;
+        if (a.zero_u) a.zero_u[o] = T(0);
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict(RestrictArgs<T> a) {
+    restrict_tile(a, blockIdx.x, gridDim.x);
 }
 
 // Neumann::restrict_to (include/neumann.h:146-252) for every Neumann face of the coarse
@@ -459,10 +480,14 @@ __device__ __forceinline__ void bc_restrict_face(const BcRestrictArgs<T>& a, int
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
-    const int fc = blockIdx.y;
+__device__ __forceinline__ void bc_restrict_tile(const BcRestrictArgs<T>& a, const int bx, const int fc, const int gx) {
     if (!a.neumann[fc]) return;
-    bc_restrict_face(a, fc, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+    bc_restrict_face(a, fc, bx * 256ll + threadIdx.x, gx * 256ll);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
+    bc_restrict_tile(a, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // ------------------------------------------------------------------------------------
@@ -680,14 +705,28 @@ __device__ __forceinline__ T half_sum(T a, T b) {
 
 // One thread: fine rows (2ic..2ic+1, 2jc..2jc+1) at one k-vector, from the coarse values
 // (ic..ic+1, jc..jc+1, kb/2..kb/2+V/2) -- each coarse value is loaded once per thread.
+template <typename T>
+struct ProlongArgs {
+    const T* uc;
+    Geom Gc;
+    T* u;
+    T* r;
+    Geom Gf;
+};
+
 template <typename T, bool ADD>
-__global__ void __launch_bounds__(256) k_prolong(const T* __restrict__ uc, Geom Gc, T* u, T* r, Geom Gf) {
+__device__ __forceinline__ void prolong_tile(const ProlongArgs<T>& a, const int bx, const int by) {
     constexpr int V = VecT<T>::V;
     constexpr int NQ = V / 2 + 1;
+    const T* __restrict__ uc = a.uc;
+    const Geom& Gc = a.Gc;
+    const Geom& Gf = a.Gf;
+    T* u = a.u;
+    T* r = a.r;
     const int nv = (Gf.nz + V - 1) / V;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = bx * 256 + threadIdx.x;
     if (t >= Gc.ny * nv) return;
-    const int ic = blockIdx.y;
+    const int ic = by;
     const int jc = t / nv;
     const int kb = (t - jc * nv) * V;  // even
     const bool i_odd_ok = 2 * ic + 1 < Gf.nx, j_odd_ok = 2 * jc + 1 < Gf.ny;
@@ -707,14 +746,18 @@ __global__ void __launch_bounds__(256) k_prolong(const T* __restrict__ uc, Geom 
     for (int e = 0; e < V; e++)
         if (kb + e < Gf.nz) ins |= 1u << e;
     const unsigned full = (1u << V) - 1u;
+    // the four fine rows' values, all loads issued before any store
+    T ev[2][2][V];
+    T uv[2][2][V];
+    bool ok[2][2];
+    long long pp[2][2];
+    unsigned insd[2][2];
 #pragma unroll
-    for (int ip = 0; ip < 2; ip++) {
-        if (ip && !i_odd_ok) continue;
-        const int i = 2 * ic + ip;
+    for (int ip = 0; ip < 2; ip++)
 #pragma unroll
         for (int jp = 0; jp < 2; jp++) {
-            if (jp && !j_odd_ok) continue;
-            const int j = 2 * jc + jp;
+            ok[ip][jp] = (!ip || i_odd_ok) && (!jp || j_odd_ok);
+            const int i = 2 * ic + ip, j = 2 * jc + jp;
             // x pass (odd i: midpoint of the two coarse planes), then y pass, per coarse z
             T yv[NQ];
 #pragma unroll
@@ -726,42 +769,61 @@ __global__ void __launch_bounds__(256) k_prolong(const T* __restrict__ uc, Geom 
                 }
                 yv[q] = jp ? half_sum(x0, x1) : x0;
             }
-            T ev[V];
 #pragma unroll
-            for (int e = 0; e < V; e++) ev[e] = (e & 1) ? half_sum(yv[e >> 1], yv[(e >> 1) + 1]) : yv[e >> 1];
-            const long long p = (long long)i * Gf.sx + (long long)j * Gf.sy + kb;
+            for (int e = 0; e < V; e++)
+                ev[ip][jp][e] = (e & 1) ? half_sum(yv[e >> 1], yv[(e >> 1) + 1]) : yv[e >> 1];
+            pp[ip][jp] = (long long)i * Gf.sx + (long long)j * Gf.sy + kb;
             const bool ijin = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1;
             unsigned inside = 0u;
 #pragma unroll
             for (int e = 0; e < V; e++)
                 if (ijin && kb + e >= Gf.z0 && kb + e < Gf.z1) inside |= 1u << e;
-            if (ADD) {
+            insd[ip][jp] = inside;
+            if (ADD && ok[ip][jp]) {
                 if (ins == full) {
-                    T uv[V];
-                    ldv_rw(uv, u + p);
-#pragma unroll
-                    for (int e = 0; e < V; e++) uv[e] = uv[e] + ev[e];
-                    stv(u + p, uv);
+                    ldv_rw(uv[ip][jp], u + pp[ip][jp]);
                 } else {
 #pragma unroll
-                    for (int e = 0; e < V; e++)
-                        if ((ins >> e) & 1u) u[p + e] = u[p + e] + ev[e];
-                }
-                const unsigned rm = ins & ~inside;
-#pragma unroll
-                for (int e = 0; e < V; e++)
-                    if ((rm >> e) & 1u) r[p + e] = ev[e];
-            } else {
-                if (ins == full) {
-                    stv(r + p, ev);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < V; e++)
-                        if ((ins >> e) & 1u) r[p + e] = ev[e];
+                    for (int e = 0; e < V; e++) uv[ip][jp][e] = ((ins >> e) & 1u) ? u[pp[ip][jp] + e] : T(0);
                 }
             }
         }
-    }
+#pragma unroll
+    for (int ip = 0; ip < 2; ip++)
+#pragma unroll
+        for (int jp = 0; jp < 2; jp++) {
+            if (!ok[ip][jp]) continue;
+            const long long p = pp[ip][jp];
+            if (ADD) {
+                T nv[V];
+#pragma unroll
+                for (int e = 0; e < V; e++) nv[e] = uv[ip][jp][e] + ev[ip][jp][e];
+                if (ins == full) {
+                    stv(u + p, nv);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if ((ins >> e) & 1u) u[p + e] = nv[e];
+                }
+                const unsigned rm = ins & ~insd[ip][jp];
+#pragma unroll
+                for (int e = 0; e < V; e++)
+                    if ((rm >> e) & 1u) r[p + e] = ev[ip][jp][e];
+            } else {
+                if (ins == full) {
+                    stv(r + p, ev[ip][jp]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if ((ins >> e) & 1u) r[p + e] = ev[ip][jp][e];
+                }
+            }
+        }
+}
+
+template <typename T, bool ADD>
+__global__ void __launch_bounds__(256) k_prolong(ProlongArgs<T> a) {
+    prolong_tile<T, ADD>(a, blockIdx.x, blockIdx.y);
 }
 
 // u += r over the shape (DeviceArray::add).
@@ -818,12 +880,12 @@ struct RefineArgs {
 };
 
 template <typename T, typename Ti, bool WRITE_R>
-__global__ void __launch_bounds__(256) k_refine_residual(RefineArgs<T, Ti> a) {
+__device__ __forceinline__ void refine_residual_tile(const RefineArgs<T, Ti>& a, const int bx, const int by) {
     constexpr int V = VecT<T>::V;
     const Geom& G = a.G;
     const int nv = (G.nz + V - 1) / V;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ia = blockIdx.y * a.ichunk;
+    const int t = bx * 256 + threadIdx.x;
+    const int ia = by * a.ichunk;
     const int ib = min(G.nx, ia + a.ichunk);
     unsigned long long mx = 0ull;
     if (t < G.ny * nv) {
@@ -925,12 +987,28 @@ __global__ void __launch_bounds__(256) k_refine_residual(RefineArgs<T, Ti> a) {
     block_max_to(mx, a.norm);
 }
 
+template <typename T, typename Ti, bool WRITE_R>
+__global__ void __launch_bounds__(256) k_refine_residual(RefineArgs<T, Ti> a) {
+    refine_residual_tile<T, Ti, WRITE_R>(a, blockIdx.x, blockIdx.y);
+}
+
 // u += (T) e over the relaxation bounds (e: the inner level-0 solution).
 template <typename T, typename Ti>
-__global__ void __launch_bounds__(256) k_refine_update(T* u, Geom G, const Ti* __restrict__ e, long long sxi,
-                                                       long long syi) {
+struct UpdateArgs {
+    T* u;
+    Geom G;
+    const Ti* e;
+    long long sxi, syi;
+};
+
+template <typename T, typename Ti>
+__device__ __forceinline__ void refine_update_tile(const UpdateArgs<T, Ti>& a, const int bx, const int gx) {
+    T* u = a.u;
+    const Geom& G = a.G;
+    const Ti* __restrict__ e = a.e;
+    const long long sxi = a.sxi, syi = a.syi;
     const long long n = (long long)G.nx * G.ny * G.nz;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = bx * 256ll + threadIdx.x; t < n; t += gx * 256ll) {
         const int k = (int)(t % G.nz);
         const long long q = t / G.nz;
         const int j = (int)(q % G.ny);
@@ -938,6 +1016,31 @@ __global__ void __launch_bounds__(256) k_refine_update(T* u, Geom G, const Ti* _
         if (i < G.x0 || i >= G.x1 || j < G.y0 || j >= G.y1 || k < G.z0 || k >= G.z1) continue;
         const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
         u[p] = u[p] + (T)ldg(e + (long long)i * sxi + (long long)j * syi + k);
+    }
+}
+
+template <typename T, typename Ti>
+__global__ void __launch_bounds__(256) k_refine_update(UpdateArgs<T, Ti> a) {
+    refine_update_tile(a, blockIdx.x, gridDim.x);
+}
+
+// Device-side right-hand side: a sum of separable sine modes at the grid points.
+struct SineModes {
+    int n;
+    double amp[64], wx[64], wy[64], wz[64];  // wx = kx*pi/Lx etc.
+};
+
+__global__ void __launch_bounds__(256) k_fill_sine(double* f, Geom G, double h, const SineModes* __restrict__ m) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        const double x = i * h, y = j * h, z = k * h;
+        double acc = 0.0;
+        for (int s = 0; s < m->n; s++) acc += m->amp[s] * sin(m->wx[s] * x) * sin(m->wy[s] * y) * sin(m->wz[s] * z);
+        f[(long long)i * G.sx + (long long)j * G.sy + k] = acc;
     }
 }
 

@@ -76,6 +76,12 @@ class Stats(ctypes.Structure):
                 ("kernel_launches", ctypes.c_int64)]
 
 
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("restriction", ctypes.c_int32), ("relaxation", ctypes.c_int32), ("inner_dtype", ctypes.c_int32),
+                ("cycle", ctypes.c_int32), ("nsmooth", ctypes.c_int64), ("omega", ctypes.c_double),
+                ("max_problems", ctypes.c_int64), ("device", ctypes.c_int32), ("flags", ctypes.c_uint32)]
+
+
 _lib = None
 
 
@@ -112,6 +118,17 @@ def lib():
         L.mgp_norm.argtypes = [vp, i32, i32, ctypes.POINTER(dbl)]
         L.mgp_synchronize.argtypes = [vp]
         L.mgp_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.mgp_batch_create.argtypes = [ctypes.POINTER(BatchDesc), ctypes.POINTER(vp)]
+        L.mgp_batch_destroy.argtypes = [vp]
+        L.mgp_batch_problem_bytes.argtypes = [ctypes.POINTER(BatchDesc), ctypes.POINTER(Desc), ctypes.POINTER(i64)]
+        L.mgp_batch_add.argtypes = [vp, ctypes.POINTER(Desc), ctypes.POINTER(i32)]
+        L.mgp_batch_problem.argtypes = [vp, i32, ctypes.POINTER(vp)]
+        L.mgp_batch_remove.argtypes = [vp, i32]
+        L.mgp_batch_set_active.argtypes = [vp, i32, i32]
+        L.mgp_batch_step.argtypes = [vp, ctypes.POINTER(i32)]
+        L.mgp_batch_status.argtypes = [vp, i32, ctypes.POINTER(Stats)]
+        L.mgp_batch_solve.argtypes = [vp, dbl, i64, ctypes.POINTER(i64)]
+        L.mgp_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(i64)]
         L.mgp_host_alloc.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t]
         L.mgp_host_free.argtypes = [vp]
         _lib = L
@@ -177,27 +194,26 @@ class Solver:
 
     def __init__(self, dims, levels, h, bc=(DIRICHLET,) * 6, restriction=INJECTION, relaxation=GAUSSSEIDEL,
                  dtype=F64, maxiter=100, miniter=1, tolerance=1e-6, origin=(0.0, 0.0, 0.0), device=0,
-                 strict_bc=False, flags=0):
+                 strict_bc=False, flags=0, _handle=None):
         L = lib()
-        d = Desc()
-        d.dims[:] = list(dims)
-        d.levels, d.maxiter, d.miniter, d.tolerance, d.h = levels, maxiter, miniter, tolerance, h
-        d.origin[:] = list(origin)
-        d.bc[:] = list(bc)
-        d.restriction = restriction if isinstance(restriction, int) else _RESTRICTIONS[restriction]
-        d.prolongation = TRILINEAR
-        d.relaxation = relaxation if isinstance(relaxation, int) else _RELAXATIONS[relaxation]
-        d.dtype = dtype
-        d.device = device
-        d.flags = (FLAG_STRICT_BC if strict_bc else 0) | flags
+        self._owned = _handle is None
+        d = make_desc(dims, levels, h, bc, restriction, relaxation, dtype, maxiter, miniter, tolerance, origin, device,
+                      strict_bc, flags)
+        if _handle is not None:
+            self._h = ctypes.c_void_p(_handle)
+            self._init_levels(d, levels)
+            return
         self._h = ctypes.c_void_p()
         _check(L.mgp_create(ctypes.byref(d), ctypes.byref(self._h)))
+        self._init_levels(d, levels)
+
+    def _init_levels(self, d, levels):
+        L = lib()
         self.desc = d
-        self.dtype = dtype
-        self.np_dtype = _np_dtype(dtype)
+        self.dtype = d.dtype
+        self.np_dtype = _np_dtype(d.dtype)
         self.levels = levels
         self.level = []
-        # a refinement solver exposes its FP64 level 0 only (the correction hierarchy is internal)
         for l in range(L.mgp_num_levels(self._h)):
             li = LevelInfo()
             _check(L.mgp_level_info_get(self._h, l, ctypes.byref(li)))
@@ -207,6 +223,8 @@ class Solver:
                                     tuple(tuple(li.face_shape[f]) for f in range(6))))
 
     def close(self):
+        if not getattr(self, "_owned", True):
+            return
         if getattr(self, "_h", None) and self._h.value and _lib is not None:
             _lib.mgp_destroy(self._h)
             self._h = ctypes.c_void_p()
@@ -313,6 +331,98 @@ class Solver:
         _check(lib().mgp_solve(self._h, cyc, nsmooth, omega, (ofile or "").encode(), maxtime, flags,
                                ctypes.byref(st)))
         return st
+
+
+def make_desc(dims, levels, h, bc=(DIRICHLET,) * 6, restriction=INJECTION, relaxation=GAUSSSEIDEL, dtype=F64,
+              maxiter=100, miniter=1, tolerance=1e-6, origin=(0.0, 0.0, 0.0), device=0, strict_bc=False, flags=0):
+    d = Desc()
+    d.dims[:] = list(dims)
+    d.levels, d.maxiter, d.miniter, d.tolerance, d.h = levels, maxiter, miniter, tolerance, h
+    d.origin[:] = list(origin)
+    d.bc[:] = list(bc)
+    d.restriction = restriction if isinstance(restriction, int) else _RESTRICTIONS[restriction]
+    d.prolongation = TRILINEAR
+    d.relaxation = relaxation if isinstance(relaxation, int) else _RELAXATIONS[relaxation]
+    d.dtype = dtype
+    d.device = device
+    d.flags = (FLAG_STRICT_BC if strict_bc else 0) | flags
+    return d
+
+
+class Batch:
+    """Many independent problems solved together (C ABI mgp_batch_*): every level operation
+    of every problem at the same depth runs as one persistent kernel over a (problem, tile)
+    work list.  Each problem is a refinement solver: FP64 level 0, correction hierarchy in
+    `inner_dtype`."""
+
+    def __init__(self, restriction=FULLWEIGHTING, relaxation=GAUSSSEIDEL, inner_dtype=F32, cycle="Fcycle",
+                 nsmooth=2, omega=-1.0, max_problems=256, device=0):
+        bd = BatchDesc()
+        bd.restriction = restriction if isinstance(restriction, int) else _RESTRICTIONS[restriction]
+        bd.relaxation = relaxation if isinstance(relaxation, int) else _RELAXATIONS[relaxation]
+        bd.inner_dtype = inner_dtype
+        bd.cycle = cycle if isinstance(cycle, int) else _CYCLES[cycle]
+        bd.nsmooth, bd.omega, bd.max_problems, bd.device, bd.flags = nsmooth, omega, max_problems, device, 0
+        self.bdesc = bd
+        self._h = ctypes.c_void_p()
+        _check(lib().mgp_batch_create(ctypes.byref(bd), ctypes.byref(self._h)))
+        self._views = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.mgp_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def problem_bytes(self, dims, levels, h, bc=(DIRICHLET,) * 6, strict_bc=False) -> int:
+        d = make_desc(dims, levels, h, bc, strict_bc=strict_bc)
+        out = ctypes.c_int64()
+        _check(lib().mgp_batch_problem_bytes(ctypes.byref(self.bdesc), ctypes.byref(d), ctypes.byref(out)))
+        return out.value
+
+    def add(self, dims, levels, h, bc=(DIRICHLET,) * 6, origin=(0.0, 0.0, 0.0), strict_bc=False) -> int:
+        d = make_desc(dims, levels, h, bc, self.bdesc.restriction, self.bdesc.relaxation, F64, origin=origin,
+                      device=self.bdesc.device, strict_bc=strict_bc)
+        pid = ctypes.c_int()
+        _check(lib().mgp_batch_add(self._h, ctypes.byref(d), ctypes.byref(pid)))
+        hp = ctypes.c_void_p()
+        _check(lib().mgp_batch_problem(self._h, pid.value, ctypes.byref(hp)))
+        self._views[pid.value] = Solver(dims, levels, h, bc, self.bdesc.restriction, self.bdesc.relaxation, F64,
+                                        origin=origin, _handle=hp.value)
+        return pid.value
+
+    def problem(self, pid) -> "Solver":
+        """The problem's solver (uploads, downloads, write_bc); owned by the batch."""
+        return self._views[pid]
+
+    def remove(self, pid):
+        self._views.pop(pid, None)
+        _check(lib().mgp_batch_remove(self._h, pid))
+
+    def set_active(self, pid, active=True):
+        _check(lib().mgp_batch_set_active(self._h, pid, int(active)))
+
+    def step(self) -> int:
+        n = ctypes.c_int()
+        _check(lib().mgp_batch_step(self._h, ctypes.byref(n)))
+        return n.value
+
+    def status(self, pid) -> Stats:
+        st = Stats()
+        _check(lib().mgp_batch_status(self._h, pid, ctypes.byref(st)))
+        return st
+
+    def solve(self, tol, maxiter=100) -> int:
+        k = ctypes.c_int64()
+        _check(lib().mgp_batch_solve(self._h, tol, maxiter, ctypes.byref(k)))
+        return k.value
+
+    def launches_per_step(self) -> int:
+        k = ctypes.c_int64()
+        _check(lib().mgp_batch_kernel_launches(self._h, ctypes.byref(k)))
+        return k.value
 
 
 # ----------------------------------------------------------------------------------------
