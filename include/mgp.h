@@ -253,6 +253,28 @@ int mgp_mem_info(int device, size_t* free_bytes, size_t* total_bytes);
 int mgp_fill_sine_modes(mgp_solver* s, int n_modes, const double* amp, const double* kx, const double* ky,
                         const double* kz, const double L[3]);
 
+/* Device-side right-hand side: level-0 f set to independent uniform values in [lo, hi):
+ * value(n) = lo + (hi-lo) * (splitmix64(seed + n*0x9E3779B97F4A7C15) >> 11) * 2^-53, n the
+ * point's linear index i*ny*nz + j*nz + k over the shape. */
+int mgp_fill_uniform(mgp_solver* s, uint64_t seed, double lo, double hi);
+
+/* Device-side PoissonSolver::init (include/libpoisson.h:158-171) for the reference's test
+ * problems (src/problem_definition.cpp): problem 1 sin(3x)sin(5.3y)sin(-7.8z), 2 x^3y^2z,
+ * 3 cos(xz^2)sin(y^3).  Level-0 f at every shape point, the level-0 face arrays (Dirichlet: u,
+ * Neumann: the normal derivative, as Boundary::init_by_fun samples them), u = 0, then the
+ * Dirichlet data written into u (mgp_write_bc).  Coordinates origin + index*h.  The values
+ * come from the device's sin/cos, so they may differ from a host init() in the last bit. */
+int mgp_fill_problem(mgp_solver* s, int problem);
+
+/* Error of level-0 u over the shape against another solver's level-0 u (ref != NULL, same
+ * shape) or, with ref == NULL, against the analytic solution of test problem `problem`
+ * (1..3, see mgp_fill_problem).  out[0] = max |u - v|, out[1] = sqrt(sum (u-v)^2),
+ * out[2] = sqrt(sum v^2), out[3] = max |v|. */
+int mgp_u_error(mgp_solver* s, mgp_solver* ref, int problem, double out[4]);
+/* Re-start a batch problem (after new data was loaded): active again, initial residual
+ * recomputed at the next step. */
+int mgp_batch_restart(mgp_batch* b, int id);
+
 /* Page-locked host memory for field buffers (faster uploads/downloads). */
 int mgp_host_alloc(void** p, size_t bytes);
 int mgp_host_free(void* p);

@@ -391,7 +391,15 @@ int batch_rebuild(mgp_batch* b) {
     // capture the launch list once; replayed every step while the active set is unchanged
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    // the step's last launch max-reduces each problem's residual into its slot
+    cudaError_t me = cudaMemsetAsync(b->d_norms, 0, sizeof(unsigned long long) * b->slots, b->stream);
     for (auto& L : b->launches) L.fn((const char*)b->d_items + L.offset, L.n, L.total, L.grid, b->stream);
+    if (me != cudaSuccess) {
+        cudaGraph_t g0 = nullptr;
+        cudaStreamEndCapture(b->stream, &g0);
+        if (g0) cudaGraphDestroy(g0);
+        return fail(MGP_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(me));
+    }
     cudaError_t le = cudaGetLastError();
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (le != cudaSuccess || e != cudaSuccess) {
@@ -618,6 +626,17 @@ int mgp_batch_step(mgp_batch* b, int* n_active) {
     }
     b->sched_state.clear();
     for (auto& p : b->probs) b->sched_state.push_back(p.s ? state_bits(p.s->inner) : 0);
+    return MGP_OK;
+}
+
+int mgp_batch_restart(mgp_batch* b, int id) {
+    if (!b) return fail(MGP_ERR_INVALID_ARG, "null batch");
+    BatchProblem* p = batch_find(b, id);
+    if (!p) return fail(MGP_ERR_INVALID_ARG, "no problem %d in the batch", id);
+    p->started = false;
+    p->active = true;
+    p->iters = 0;
+    b->dirty = true;
     return MGP_OK;
 }
 

@@ -1256,6 +1256,75 @@ int mgp_fill_sine_modes(mgp_solver* s, int n_modes, const double* amp, const dou
     return MGP_OK;
 }
 
+int mgp_fill_problem(mgp_solver* s, int problem) {
+    CKS(validate(s));
+    if (s->dtype != MGP_F64) return fail(MGP_ERR_INVALID_ARG, "the problem fill writes FP64 level-0 data");
+    if (problem < 1 || problem > 3) return fail(MGP_ERR_INVALID_ARG, "problem must be 1, 2 or 3");
+    DeviceGuard guard(s->device);
+    LevelState& L0 = s->lv[0];
+    ProblemFill pf{problem, s->desc.origin[0], s->desc.origin[1], s->desc.origin[2], L0.h};
+    const long long n = (long long)L0.G.nx * L0.G.ny * L0.G.nz;
+    k_fill_problem_f<<<grid_1d(s, n), kThreads, 0, s->stream>>>((double*)L0.f, (double*)u_ptr(s, 0), L0.G, pf);
+    CKS(check_launch(s));
+    for (int f = 0; f < 6; f++) {
+        const int64_t* fs = L0.face_shape[f];
+        const long long nf = fs[0] * fs[1] * fs[2];
+        k_fill_problem_face<<<grid_1d(s, nf), kThreads, 0, s->stream>>>((double*)L0.face[f], L0.G, pf, f,
+                                                                          s->face_kind[f] == MGP_NEUMANN);
+        CKS(check_launch(s));
+    }
+    if (L0.ubuf[1]) CK(cudaMemsetAsync(uprev_ptr(s, 0), 0, L0.elems * sizeof(double), s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return mgp_write_bc(s, 0);
+}
+
+int mgp_u_error(mgp_solver* s, mgp_solver* ref, int problem, double out[4]) {
+    CKS(validate(s));
+    if (!out) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
+    if (s->dtype != MGP_F64 || (ref && ref->dtype != MGP_F64)) return fail(MGP_ERR_INVALID_ARG, "FP64 solvers only");
+    LevelState& L0 = s->lv[0];
+    if (ref && (ref->lv[0].G.nx != L0.G.nx || ref->lv[0].G.ny != L0.G.ny || ref->lv[0].G.nz != L0.G.nz))
+        return fail(MGP_ERR_INVALID_ARG, "shapes differ");
+    if (!ref && (problem < 1 || problem > 3)) return fail(MGP_ERR_INVALID_ARG, "problem must be 1, 2 or 3");
+    DeviceGuard guard(s->device);
+    unsigned long long* dm = nullptr;
+    CK(cudaMallocAsync((void**)&dm, 64, s->stream));
+    cudaError_t e = cudaMemsetAsync(dm, 0, 64, s->stream);
+    ProblemFill pf{problem, s->desc.origin[0], s->desc.origin[1], s->desc.origin[2], L0.h};
+    const long long n = (long long)L0.G.nx * L0.G.ny * L0.G.nz;
+    if (e == cudaSuccess) {
+        k_u_error<<<grid_1d(s, n), kThreads, 0, s->stream>>>((const double*)u_ptr(s, 0),
+                                                            ref ? (const double*)u_ptr(ref, 0) : nullptr, L0.G,
+                                                            ref ? ref->lv[0].G : L0.G, pf, dm, (double*)(dm + 2));
+        e = cudaGetLastError();
+        s->launches++;
+    }
+    unsigned long long h[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, dm, 32, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(dm, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(MGP_ERR_CUDA, "u error: %s", cudaGetErrorString(e));
+    double v[4];
+    memcpy(v, h, 32);
+    out[0] = v[0];
+    out[1] = std::sqrt(v[2]);
+    out[2] = std::sqrt(v[3]);
+    out[3] = v[1];
+    return MGP_OK;
+}
+
+int mgp_fill_uniform(mgp_solver* s, uint64_t seed, double lo, double hi) {
+    CKS(validate(s));
+    if (s->dtype != MGP_F64) return fail(MGP_ERR_INVALID_ARG, "the uniform fill writes an FP64 right-hand side");
+    DeviceGuard guard(s->device);
+    LevelState& L0 = s->lv[0];
+    const long long n = (long long)L0.G.nx * L0.G.ny * L0.G.nz;
+    k_fill_uniform<<<grid_1d(s, n), kThreads, 0, s->stream>>>((double*)L0.f, L0.G, (unsigned long long)seed, lo, hi);
+    CKS(check_launch(s));
+    CK(cudaStreamSynchronize(s->stream));
+    return MGP_OK;
+}
+
 int mgp_host_alloc(void** p, size_t bytes) {
     if (!p) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
     CK(cudaMallocHost(p, bytes));

@@ -1044,6 +1044,142 @@ __global__ void __launch_bounds__(256) k_fill_sine(double* f, Geom G, double h, 
     }
 }
 
+// The reference's test problems (src/problem_definition.cpp) on the device.
+__device__ __forceinline__ double prob_u(int p, double x, double y, double z) {
+    switch (p) {
+        case 1: return sin(3.0 * x) * sin(5.3 * y) * sin(-7.8 * z);
+        case 2: return x * x * x * y * y * z;
+        default: return cos(x * z * z) * sin(y * y * y);
+    }
+}
+__device__ __forceinline__ double prob_f(int p, double x, double y, double z) {
+    switch (p) {
+        case 1: return -(3.0 * 3.0 + 5.3 * 5.3 + (-7.8) * (-7.8)) * sin(3.0 * x) * sin(5.3 * y) * sin(-7.8 * z);
+        case 2: return 2.0 * x * x * x * z + 6.0 * x * y * y * z;
+        default:
+            return ((-4.0 * x * x * z * z - 9.0 * y * y * y * y - z * z * z * z) * sin(y * y * y) +
+                    6.0 * y * cos(y * y * y)) * cos(x * z * z) -
+                   2.0 * x * sin(x * z * z) * sin(y * y * y);
+    }
+}
+__device__ __forceinline__ double prob_d(int p, int axis, double x, double y, double z) {
+    if (p == 1) {
+        if (axis == 0) return 3.0 * cos(3.0 * x) * sin(5.3 * y) * sin(-7.8 * z);
+        if (axis == 1) return 5.3 * sin(3.0 * x) * cos(5.3 * y) * sin(-7.8 * z);
+        return -7.8 * sin(3.0 * x) * sin(5.3 * y) * cos(-7.8 * z);
+    }
+    if (p == 2) {
+        if (axis == 0) return 3.0 * x * x * y * y * z;
+        if (axis == 1) return 2.0 * x * x * x * y * z;
+        return x * x * x * y * y;
+    }
+    if (axis == 0) return -z * z * sin(x * z * z) * sin(y * y * y);
+    if (axis == 1) return 3.0 * cos(x * z * z) * y * y * cos(y * y * y);
+    return -2 * x * z * sin(x * z * z) * sin(y * y * y);
+}
+
+struct ProblemFill {
+    int problem;
+    double x0, y0, z0, h;
+};
+
+__global__ void __launch_bounds__(256) k_fill_problem_f(double* f, double* u, Geom G, ProblemFill pf) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        const long long o = (long long)i * G.sx + (long long)j * G.sy + k;
+        f[o] = prob_f(pf.problem, pf.x0 + ((double)i) * pf.h, pf.y0 + ((double)j) * pf.h, pf.z0 + ((double)k) * pf.h);
+        u[o] = 0.0;
+    }
+}
+
+// Boundary::init_by_fun (include/boundary.h:81-111) for one face: Dirichlet faces sample u,
+// Neumann faces the derivative normal to the face (neumann.h:63-79).
+__global__ void __launch_bounds__(256) k_fill_problem_face(double* g, Geom G, ProblemFill pf, int fc, int neumann) {
+    int n0, n1;
+    if (fc == F_EAST || fc == F_WEST) { n0 = G.ny; n1 = G.nz; }
+    else if (fc == F_NORTH || fc == F_SOUTH) { n0 = G.nx; n1 = G.nz; }
+    else { n0 = G.nx; n1 = G.ny; }
+    const long long n = (long long)n0 * n1;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t % n1), a0 = (int)(t / n1);
+        double i, j, k;
+        if (fc == F_EAST || fc == F_WEST) { i = fc == F_EAST ? G.nx - 1 : 0; j = a0; k = b; }
+        else if (fc == F_NORTH || fc == F_SOUTH) { i = a0; j = fc == F_NORTH ? G.ny - 1 : 0; k = b; }
+        else { i = a0; j = b; k = fc == F_TOP ? G.nz - 1 : 0; }
+        const double x = pf.x0 + i * pf.h, y = pf.y0 + j * pf.h, z = pf.z0 + k * pf.h;
+        const int axis = (fc == F_EAST || fc == F_WEST) ? 0 : (fc == F_NORTH || fc == F_SOUTH) ? 1 : 2;
+        g[t] = neumann ? prob_d(pf.problem, axis, x, y, z) : prob_u(pf.problem, x, y, z);
+    }
+}
+
+// Error reduction: out[0] max|u-v| (bits), out[1] sum (u-v)^2, out[2] sum v^2, out[3] max|v|.
+__global__ void __launch_bounds__(256) k_u_error(const double* __restrict__ u, const double* __restrict__ v, Geom G,
+                                                 Geom Gv, ProblemFill pf, unsigned long long* mx, double* sums) {
+    __shared__ double red[2][8];
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    unsigned long long m0 = 0, m1 = 0;
+    double s1 = 0.0, s2 = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        const double a = u[(long long)i * G.sx + (long long)j * G.sy + k];
+        const double b = v ? v[(long long)i * Gv.sx + (long long)j * Gv.sy + k]
+                           : prob_u(pf.problem, pf.x0 + i * pf.h, pf.y0 + j * pf.h, pf.z0 + k * pf.h);
+        const double d = a - b;
+        m0 = max(m0, abs_bits(d));
+        m1 = max(m1, abs_bits(b));
+        s1 += d * d;
+        s2 += b * b;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][w] = s1;
+        red[1][w] = s2;
+    }
+    block_max_to(m0, mx);
+    block_max_to(m1, mx + 1);
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
+            a += red[0][q];
+            b += red[1][q];
+        }
+        atomicAdd(sums, a);
+        atomicAdd(sums + 1, b);
+    }
+}
+
+// splitmix64 (Steele, Lea, Flood 2014) as a counter-based generator.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__global__ void __launch_bounds__(256) k_fill_uniform(double* f, Geom G, unsigned long long seed, double lo, double hi) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        const unsigned long long r = splitmix64(seed + (unsigned long long)t * 0x9E3779B97F4A7C15ull);
+        const double u01 = (double)(r >> 11) * 0x1.0p-53;
+        f[(long long)i * G.sx + (long long)j * G.sy + k] = lo + (hi - lo) * u01;
+    }
+}
+
 // Dirichlet::write_to (include/dirichlet.h:50-93): one face into its boundary plane.
 template <typename T>
 __global__ void __launch_bounds__(256) k_write_face(T* u, Geom G, const T* __restrict__ g, int fc) {

@@ -129,6 +129,13 @@ def lib():
         L.mgp_batch_status.argtypes = [vp, i32, ctypes.POINTER(Stats)]
         L.mgp_batch_solve.argtypes = [vp, dbl, i64, ctypes.POINTER(i64)]
         L.mgp_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(i64)]
+        L.mgp_mem_info.argtypes = [i32, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+        dp = ctypes.POINTER(dbl)
+        L.mgp_fill_sine_modes.argtypes = [vp, i32, dp, dp, dp, dp, dp]
+        L.mgp_fill_uniform.argtypes = [vp, ctypes.c_uint64, dbl, dbl]
+        L.mgp_fill_problem.argtypes = [vp, i32]
+        L.mgp_u_error.argtypes = [vp, vp, i32, ctypes.POINTER(dbl)]
+        L.mgp_batch_restart.argtypes = [vp, i32]
         L.mgp_host_alloc.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t]
         L.mgp_host_free.argtypes = [vp]
         _lib = L
@@ -138,6 +145,13 @@ def lib():
 def _check(st: int):
     if st != OK:
         raise MgpError(st, lib().mgp_last_error().decode())
+
+
+def mem_info(device=0):
+    """(free, total) device bytes."""
+    f, t = ctypes.c_size_t(), ctypes.c_size_t()
+    _check(lib().mgp_mem_info(device, ctypes.byref(f), ctypes.byref(t)))
+    return f.value, t.value
 
 
 def device_count() -> int:
@@ -311,6 +325,28 @@ class Solver:
     def synchronize(self):
         _check(lib().mgp_synchronize(self._h))
 
+    def fill_sine_modes(self, amp, kx, ky, kz, L):
+        """Device-side level-0 f = sum_m amp sin(kx pi x/Lx) sin(ky pi y/Ly) sin(kz pi z/Lz)."""
+        n = len(amp)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (amp, kx, ky, kz, L)]
+        ptr = [a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in arrs]
+        _check(lib().mgp_fill_sine_modes(self._h, n, *ptr))
+
+    def fill_problem(self, problem):
+        """Device-side init() for the reference's test problems 1, 2, 3 (f, faces, u = 0 + Dirichlet data)."""
+        _check(lib().mgp_fill_problem(self._h, problem))
+
+    def u_error(self, ref=None, problem=0):
+        """(max-abs error, relative L2 error, max |v|) of level-0 u against `ref` (a Solver) or the
+        analytic solution of test problem `problem`."""
+        out = (ctypes.c_double * 4)()
+        _check(lib().mgp_u_error(self._h, ref._h if ref is not None else None, problem, out))
+        return out[0], (out[1] / out[2] if out[2] > 0 else float("nan")), out[3]
+
+    def fill_uniform(self, seed, lo=-1.0, hi=1.0):
+        """Device-side level-0 f: independent uniform values in [lo, hi) (splitmix64 counter)."""
+        _check(lib().mgp_fill_uniform(self._h, int(seed) & (2 ** 64 - 1), lo, hi))
+
     @property
     def stream_handle(self) -> int:
         """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
@@ -400,6 +436,9 @@ class Batch:
     def remove(self, pid):
         self._views.pop(pid, None)
         _check(lib().mgp_batch_remove(self._h, pid))
+
+    def restart(self, pid):
+        _check(lib().mgp_batch_restart(self._h, pid))
 
     def set_active(self, pid, active=True):
         _check(lib().mgp_batch_set_active(self._h, pid, int(active)))

@@ -1,0 +1,186 @@
+"""Continuous-batching solve server on one GPU (built on mgp.Batch).
+
+Requests (grid dims, boundary kinds, a right-hand side given by sine modes, tolerance)
+arrive over time.  The server loop:
+
+* admits arrived requests while the device has memory for them (free HBM from
+  cudaMemGetInfo minus a reserve, per-problem bytes from mgp_batch_problem_bytes) and the
+  batch has a free slot; an admitted request's hierarchy stays resident until it finishes,
+  and its right-hand side is generated on the device;
+* runs one batched refinement step (mgp_batch_step) for every resident request -- each
+  level operation of every request is one persistent kernel over a (request, tile) work
+  list, so requests of different sizes share launches;
+* retires requests whose FP64 relative residual ||r||inf/||f||inf is below their
+  tolerance: the solution comes back to the host and the slot and memory free up.
+
+Requests that arrive while others are on the GPU join at the next step boundary (continuous
+batching, not a queue in front of a one-at-a-time solver).  Latency = finish - arrival.
+"""
+from __future__ import annotations
+
+import collections
+import hashlib
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import F32, F64, FULLWEIGHTING, GAUSSSEIDEL, Batch, mem_info
+
+KINDS = ("dirichlet", "neumann", "mixed")
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float                  # seconds after the start of the stream
+    dims: tuple
+    levels: int
+    h: float
+    bc: tuple                       # requested kinds, N S E W T B (0 Dirichlet, 1 Neumann)
+    kind: str
+    amp: np.ndarray
+    kx: np.ndarray
+    ky: np.ndarray
+    kz: np.ndarray
+    tol: float = 1e-8
+    admitted: float = float("nan")
+    finished: float = float("nan")
+    iterations: int = 0
+    rel_res: float = float("nan")
+    digest: str = ""
+    solution: np.ndarray | None = field(default=None, repr=False)
+
+    @property
+    def lengths(self):
+        return tuple((n - 1) * self.h for n in self.dims)
+
+    @property
+    def dof(self):
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+
+def make_request(rid: int, arrival: float, seed: int, kmin=5, kmax=9, tol=1e-8, rng=None, kmax_z=None) -> Request:
+    """Box sides 2^k+1 (k uniform in [kmin, kmax] independently per axis, z at most kmax_z),
+    levels down to a
+    5-point coarsest side, boundary kind uniform over Dirichlet / Neumann (the reference's
+    default {N,N,N,N,D,D}) / mixed (random per face, top and bottom alike so that the
+    red-black colouring stays well defined), zero boundary data, and a right-hand side of 8
+    sine modes with wavenumbers uniform in 1..8 and N(0,1) amplitudes from the request's seed."""
+    rng = rng or np.random.default_rng((seed, rid, 1))
+    k = rng.integers(kmin, kmax + 1, size=3)
+    if kmax_z is not None:
+        k[2] = rng.integers(kmin, min(kmax, kmax_z) + 1)
+    dims = tuple(int(2 ** kk + 1) for kk in k)
+    levels = int(k.min()) - 1
+    kind = KINDS[int(rng.integers(0, 3))]
+    if kind == "dirichlet":
+        bc = (0,) * 6
+    elif kind == "neumann":
+        bc = (1, 1, 1, 1, 0, 0)
+    else:
+        ns, ew = rng.integers(0, 2, size=4), int(rng.integers(0, 2))
+        bc = (int(ns[0]), int(ns[1]), int(ns[2]), int(ns[3]), ew, ew)
+    mr = np.random.default_rng((seed, rid, 2))
+    return Request(rid, arrival, dims, levels, 1.0 / (max(dims) - 1), bc, kind, mr.standard_normal(8),
+                   mr.integers(1, 9, size=8).astype(np.float64), mr.integers(1, 9, size=8).astype(np.float64),
+                   mr.integers(1, 9, size=8).astype(np.float64), tol)
+
+
+def make_stream(n: int, rate: float, seed: int = 0, **kw) -> list:
+    """Open-loop Poisson arrivals at `rate` requests/s."""
+    rng = np.random.default_rng((seed, 0))
+    t = 0.0
+    out = []
+    for rid in range(n):
+        t += rng.exponential(1.0 / rate)
+        out.append(make_request(rid, t, seed, **kw))
+    return out
+
+
+class Server:
+    def __init__(self, inner=F32, max_batch=64, reserve_bytes=4 << 30, device=0, max_steps=200,
+                 keep_solutions=False, nsmooth=2):
+        self.batch = Batch(FULLWEIGHTING, GAUSSSEIDEL, inner, "Fcycle", nsmooth, max_problems=max_batch,
+                           device=device)
+        self.max_batch = max_batch
+        self.reserve = reserve_bytes
+        self.device = device
+        self.max_steps = max_steps
+        self.keep = keep_solutions
+        self.steps = 0
+        self.batch_sizes = []
+
+    def close(self):
+        self.batch.close()
+
+    def _admit(self, req: Request, now: float) -> bool:
+        need = self.batch.problem_bytes(req.dims, req.levels, req.h, req.bc)
+        free, _ = mem_info(self.device)
+        if free - need < self.reserve:
+            return False
+        pid = self.batch.add(req.dims, req.levels, req.h, req.bc)
+        s = self.batch.problem(pid)
+        s.fill_sine_modes(req.amp, req.kx, req.ky, req.kz, req.lengths)
+        req.admitted = now
+        self._active[pid] = req
+        return True
+
+    def _retire(self, pid: int, req: Request, now: float):
+        st = self.batch.status(pid)
+        req.iterations, req.rel_res = int(st.iterations), st.rel_res
+        u = self.batch.problem(pid).download("u", 0)
+        req.digest = hashlib.sha256(u.tobytes()).hexdigest()[:16]
+        if self.keep:
+            req.solution = u
+        self.batch.remove(pid)
+        req.finished = now
+
+    def run(self, requests, time_scale: float = 1.0, clock=time.perf_counter) -> dict:
+        """Serve `requests` (sorted by arrival); arrival times are multiplied by time_scale."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        waiting = collections.deque()
+        self._active = {}
+        t0 = clock()
+        while pending or waiting or self._active:
+            now = clock() - t0
+            while pending and pending[0].arrival * time_scale <= now:
+                waiting.append(pending.popleft())
+            while waiting and len(self._active) < self.max_batch and self._admit(waiting[0], now):
+                waiting.popleft()
+            if not self._active:
+                if waiting:
+                    raise RuntimeError(f"request {waiting[0].rid} {waiting[0].dims} does not fit on the device")
+                if pending:
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival * time_scale - now)))
+                continue
+            self.batch.step()
+            self.steps += 1
+            self.batch_sizes.append(len(self._active))
+            now = clock() - t0
+            for pid, req in list(self._active.items()):
+                st = self.batch.status(pid)
+                if st.rel_res < req.tol or st.iterations >= self.max_steps:
+                    self._retire(pid, req, clock() - t0)
+                    del self._active[pid]
+        return summarize(requests, time_scale, self.steps, self.batch_sizes)
+
+
+def summarize(requests, time_scale, steps, batch_sizes) -> dict:
+    lat = np.array([(r.finished - r.arrival * time_scale) for r in requests])
+    span = max(r.finished for r in requests) - min(r.arrival * time_scale for r in requests)
+    dof = sum(r.dof for r in requests)
+    return {
+        "requests": len(requests),
+        "p50_ms": float(np.percentile(lat, 50) * 1e3),
+        "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "mean_ms": float(lat.mean() * 1e3),
+        "solves_per_s": len(requests) / span,
+        "dof_per_s": dof / span,
+        "span_s": span,
+        "converged": int(sum(r.rel_res < r.tol for r in requests)),
+        "mean_iterations": float(np.mean([r.iterations for r in requests])),
+        "steps": steps,
+        "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
+        "max_batch_seen": int(max(batch_sizes)) if batch_sizes else 0,
+    }
