@@ -275,6 +275,24 @@ int mgp_u_error(mgp_solver* s, mgp_solver* ref, int problem, double out[4]);
  * recomputed at the next step. */
 int mgp_batch_restart(mgp_batch* b, int id);
 
+/* Max-norm (max |a|, as mgp_norm returns it) of a caller-owned device array of
+ * shape[0] x shape[1] x shape[2] points of type dtype (MGP_F64 double, MGP_F32 float), point
+ * (i,j,k) at a[i*stride[0] + j*stride[1] + k] (strides in elements), computed on `device`
+ * on `stream` (a cudaStream_t, NULL = default stream); waits for the stream and writes the
+ * norm to *out.  No counterpart in the reference: it is a variant of mgp_norm
+ * (DeviceArray<T>::infinity_norm, include/devicearray.h:198-240) for callers that must not
+ * allocate device memory.  It allocates nothing: its scratch is a static 256 KB device array.
+ *  - At most 268435456 (2^28) points; larger shapes return MGP_ERR_INVALID_ARG.
+ *  - The first call on a device looks up the scratch array's address
+ *    (cudaGetSymbolAddress); make that first call (an empty shape does only this setup)
+ *    before any stream capture on that device.
+ *  - Nothing has to be zeroed first; every call rewrites the scratch it reads.
+ *  - Calls on the same device share the scratch: calls that overlap in time (other host
+ *    threads, or work still running on another stream) race and give wrong results.
+ *    Order them on the host. */
+int mgp_norm_device(int device, const void* a, int dtype, const int64_t shape[3], const int64_t stride[2],
+                    void* stream, double* out);
+
 /* Page-locked host memory for field buffers (faster uploads/downloads). */
 int mgp_host_alloc(void** p, size_t bytes);
 int mgp_host_free(void* p);

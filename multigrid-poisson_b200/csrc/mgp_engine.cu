@@ -1338,3 +1338,4 @@ int mgp_host_free(void* p) {
 }  // extern "C"
 
 #include "mgp_batch.cuh"
+#include "mgp_norm_static.cuh"
