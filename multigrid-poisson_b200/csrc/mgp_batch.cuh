@@ -27,6 +27,7 @@ struct BatchItem {
 
 template <typename Args, typename Tile>
 __global__ void __launch_bounds__(256) kb_run(const BatchItem<Args>* __restrict__ items, int n, int total) {
+    pdl_begin();
     for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
         int lo = 0, hi = n - 1;  // last item whose tile_start <= tile
         while (lo < hi) {
@@ -85,7 +86,8 @@ struct BatchLaunch {
 
 template <typename Tile>
 void launch_items(const void* items, int n, int total, int grid, cudaStream_t st) {
-    kb_run<typename Tile::Args, Tile><<<grid, kThreads, 0, st>>>((const BatchItem<typename Tile::Args>*)items, n, total);
+    launch_pdl(kb_run<typename Tile::Args, Tile>, dim3(grid), dim3(kThreads), 0, st,
+               (const BatchItem<typename Tile::Args>*)items, n, total);
 }
 
 struct ScheduleBuilder {

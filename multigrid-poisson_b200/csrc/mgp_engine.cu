@@ -18,10 +18,12 @@
 #include <functional>
 #include <iomanip>
 #include <iostream>
+#include <cstdlib>
 #include <map>
 #include <new>
 #include <string>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "mgp.h"
@@ -153,6 +155,38 @@ int check_launch(mgp_solver* s) {
     return MGP_OK;
 }
 
+// Programmatic dependent launches (the kernels call pdl_begin first); MGP_PDL=0 launches
+// them in ordinary stream order instead.
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("MGP_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Act>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Act&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...);
+}
+
+template <typename... KArgs, typename... Act>
+int launch_k(mgp_solver* s, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Act&&... args) {
+    const cudaError_t e = launch_pdl(kernel, grid, block, smem, s->stream, std::forward<Act>(args)...);
+    if (e != cudaSuccess) return fail(MGP_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+    return check_launch(s);
+}
+
 // Blocks of `kernel` resident per SM (256 threads, static shared memory only).
 template <typename K>
 int resident_blocks(K kernel) {
@@ -228,9 +262,8 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
     dim3 grid(bx, chunks);
-    if (OP == OP_RESIDUAL && norm) k_stencil<T, OP, true><<<grid, kThreads, 0, s->stream>>>(a);
-    else k_stencil<T, OP, false><<<grid, kThreads, 0, s->stream>>>(a);
-    return check_launch(s);
+    if (OP == OP_RESIDUAL && norm) return launch_k(s, k_stencil<T, OP, true>, grid, dim3(kThreads), 0, a);
+    return launch_k(s, k_stencil<T, OP, false>, grid, dim3(kThreads), 0, a);
 }
 
 template <typename T>
@@ -292,8 +325,7 @@ template <typename T>
 int restrict_t(mgp_solver* s, int l, bool zero_coarse_u) {
     long long n = 0;
     RestrictArgs<T> a = restrict_args<T>(s, l, zero_coarse_u, &n);
-    k_restrict<T><<<grid_1d(s, n), kThreads, 0, s->stream>>>(a);
-    return check_launch(s);
+    return launch_k(s, k_restrict<T>, dim3(grid_1d(s, n)), dim3(kThreads), 0, a);
 }
 
 template <typename T>
@@ -311,8 +343,7 @@ int restrict_bc_t(mgp_solver* s, int l) {
     for (int f = 0; f < 6; f++)
         nmax = std::max(nmax, (long long)(C.face_shape[f][0] * C.face_shape[f][1] * C.face_shape[f][2]));
     dim3 grid((unsigned)std::max(1ll, std::min((nmax + kThreads - 1) / kThreads, 4096ll)), 6);
-    k_restrict_bc<T><<<grid, kThreads, 0, s->stream>>>(a);
-    return check_launch(s);
+    return launch_k(s, k_restrict_bc<T>, grid, dim3(kThreads), 0, a);
 }
 
 template <typename T, bool ADD>
@@ -323,16 +354,14 @@ int prolong_t(mgp_solver* s, int l) {
     const int rows = C.G.ny * ((F.G.nz + V - 1) / V);  // one thread per coarse (j) row x fine k-vector
     dim3 grid((rows + kThreads - 1) / kThreads, C.G.nx);
     ProlongArgs<T> a{(const T*)u_ptr(s, l + 1), C.G, (T*)u_ptr(s, l), (T*)F.r, F.G};
-    k_prolong<T, ADD><<<grid, kThreads, 0, s->stream>>>(a);
-    return check_launch(s);
+    return launch_k(s, k_prolong<T, ADD>, grid, dim3(kThreads), 0, a);
 }
 
 template <typename T>
 int add_t(mgp_solver* s, int l) {
     LevelState& L = s->lv[l];
     const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
-    k_add<T><<<grid_1d(s, n), kThreads, 0, s->stream>>>((T*)u_ptr(s, l), (const T*)L.r, L.G);
-    return check_launch(s);
+    return launch_k(s, k_add<T>, dim3(grid_1d(s, n)), dim3(kThreads), 0, (T*)u_ptr(s, l), (const T*)L.r, L.G);
 }
 
 template <typename T>
@@ -345,8 +374,7 @@ template <typename T>
 int norm_t(mgp_solver* s, const void* a, int l, unsigned long long* out) {
     LevelState& L = s->lv[l];
     const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
-    k_norm<T><<<grid_1d(s, n), kThreads, 0, s->stream>>>((const T*)a, L.G, out);
-    return check_launch(s);
+    return launch_k(s, k_norm<T>, dim3(grid_1d(s, n)), dim3(kThreads), 0, (const T*)a, L.G, out);
 }
 
 template <typename T>
@@ -418,8 +446,7 @@ int coarse_setup_fused_t(mgp_solver* s, int l) {
         extra = 6 * a.bc_blocks_per_face;
     }
     const size_t smem = (size_t)3 * rows * (tkv * V) * sizeof(T);
-    k_resid_restrict<T><<<a.main_blocks + extra, dim3(tkv, rows), smem, s->stream>>>(a);
-    return check_launch(s);
+    return launch_k(s, k_resid_restrict<T>, dim3(a.main_blocks + extra), dim3(tkv, rows), smem, a);
 }
 
 // The three-kernel form: residual (r stored), restriction with u_{l+1} = 0 fused, Neumann
@@ -549,9 +576,8 @@ int refine_residual_t(mgp_solver* s, bool write_r) {
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
     CK(cudaMemsetAsync(s->d_norm, 0, sizeof(unsigned long long), s->stream));
-    if (write_r) k_refine_residual<double, Ti, true><<<dim3(bx, chunks), kThreads, 0, s->stream>>>(a);
-    else k_refine_residual<double, Ti, false><<<dim3(bx, chunks), kThreads, 0, s->stream>>>(a);
-    return check_launch(s);
+    if (write_r) return launch_k(s, k_refine_residual<double, Ti, true>, dim3(bx, chunks), dim3(kThreads), 0, a);
+    return launch_k(s, k_refine_residual<double, Ti, false>, dim3(bx, chunks), dim3(kThreads), 0, a);
 }
 
 template <typename Ti>
@@ -561,8 +587,7 @@ int refine_update_t(mgp_solver* s) {
     LevelState& I = in->lv[0];
     const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
     UpdateArgs<double, Ti> a{(double*)u_ptr(s, 0), L.G, (const Ti*)u_ptr(in, 0), I.G.sx, I.G.sy};
-    k_refine_update<double, Ti><<<grid_1d(s, n), kThreads, 0, s->stream>>>(a);
-    return check_launch(s);
+    return launch_k(s, k_refine_update<double, Ti>, dim3(grid_1d(s, n)), dim3(kThreads), 0, a);
 }
 
 int refine_residual(mgp_solver* s, bool write_r) {
@@ -579,7 +604,7 @@ int launch_refine_step(mgp_solver* s, int cycle, int64_t ns, double omega) {
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
         const uint64_t pre = state_bits(in);
-        const int64_t l0 = s->launches + in->launches;
+        const int64_t s0 = s->launches, i0 = in->launches;
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         int st;
@@ -594,7 +619,9 @@ int launch_refine_step(mgp_solver* s, int cycle, int64_t ns, double omega) {
         cudaError_t e = cudaStreamEndCapture(s->stream, &g);
         GraphEntry ge;
         ge.post_state = state_bits(in);
-        ge.kernels = s->launches + in->launches - l0;
+        ge.kernels = (s->launches - s0) + (in->launches - i0);
+        s->launches = s0;  // the capture launched nothing; replays count the graph's kernels
+        in->launches = i0;
         set_state_bits(in, pre);
         if (st != MGP_OK || e != cudaSuccess) {
             if (g) cudaGraphDestroy(g);

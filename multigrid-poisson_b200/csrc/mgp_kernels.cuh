@@ -35,6 +35,16 @@ struct Faces {
     const T* g[6];  // dense face arrays, reference face layout
 };
 
+// Programmatic dependent launch.  Every kernel of a cycle is launched with programmatic
+// stream serialisation and releases its dependents as soon as it starts: the next kernel's
+// CTAs are scheduled on whatever this grid leaves free (grids are dispatched in order) and
+// block in pdl_begin() until this grid has completed and its writes are visible.  The launch
+// latency between dependent kernels is hidden behind the running grid.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n");
+}
+
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) {
     return __ldg(p);
@@ -360,6 +370,7 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
 
 template <typename T, int OP, bool NORM>
 __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
+    pdl_begin();
     stencil_tile<T, OP, NORM>(a, blockIdx.x, blockIdx.y);
 }
 
@@ -427,6 +438,7 @@ __device__ __forceinline__ void restrict_tile(const RestrictArgs<T>& a, const in
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_restrict(RestrictArgs<T> a) {
+    pdl_begin();
     restrict_tile(a, blockIdx.x, gridDim.x);
 }
 
@@ -487,6 +499,7 @@ __device__ __forceinline__ void bc_restrict_tile(const BcRestrictArgs<T>& a, con
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
+    pdl_begin();
     bc_restrict_tile(a, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
@@ -520,6 +533,7 @@ struct RRArgs {
 
 template <typename T>
 __global__ void __launch_bounds__(512) k_resid_restrict(RRArgs<T> a) {
+    pdl_begin();
     if ((int)blockIdx.x >= a.main_blocks) {
         const int b = blockIdx.x - a.main_blocks;
         const int fc = b / a.bc_blocks_per_face;
@@ -823,12 +837,14 @@ __device__ __forceinline__ void prolong_tile(const ProlongArgs<T>& a, const int 
 
 template <typename T, bool ADD>
 __global__ void __launch_bounds__(256) k_prolong(ProlongArgs<T> a) {
+    pdl_begin();
     prolong_tile<T, ADD>(a, blockIdx.x, blockIdx.y);
 }
 
 // u += r over the shape (DeviceArray::add).
 template <typename T>
 __global__ void __launch_bounds__(256) k_add(T* u, const T* __restrict__ r, Geom G) {
+    pdl_begin();
     const long long n = (long long)G.nx * G.ny * G.nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % G.nz);
@@ -843,6 +859,7 @@ __global__ void __launch_bounds__(256) k_add(T* u, const T* __restrict__ r, Geom
 // max |a| over the shape (DeviceArray::infinity_norm).
 template <typename T>
 __global__ void __launch_bounds__(256) k_norm(const T* __restrict__ a, Geom G, unsigned long long* out) {
+    pdl_begin();
     const long long n = (long long)G.nx * G.ny * G.nz;
     unsigned long long mx = 0ull;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -989,6 +1006,7 @@ __device__ __forceinline__ void refine_residual_tile(const RefineArgs<T, Ti>& a,
 
 template <typename T, typename Ti, bool WRITE_R>
 __global__ void __launch_bounds__(256) k_refine_residual(RefineArgs<T, Ti> a) {
+    pdl_begin();
     refine_residual_tile<T, Ti, WRITE_R>(a, blockIdx.x, blockIdx.y);
 }
 
@@ -1021,6 +1039,7 @@ __device__ __forceinline__ void refine_update_tile(const UpdateArgs<T, Ti>& a, c
 
 template <typename T, typename Ti>
 __global__ void __launch_bounds__(256) k_refine_update(UpdateArgs<T, Ti> a) {
+    pdl_begin();
     refine_update_tile(a, blockIdx.x, gridDim.x);
 }
 
