@@ -106,6 +106,8 @@ struct mgp_solver {
     std::vector<LevelState> lv;
     unsigned long long* d_norm = nullptr;  // [0] scratch for max-norms
     unsigned long long* h_norm = nullptr;  // pinned read-back
+    void* stage = nullptr;                 // device copy of a host-layout field (large transfers)
+    size_t stage_bytes = 0;
     std::map<std::tuple<int, int64_t, uint64_t, uint64_t>, GraphEntry> graphs;
     bool capturing = false;
     int64_t launches = 0;  // kernels launched on this solver (graph replays count their nodes)
@@ -648,10 +650,81 @@ int validate_level(const mgp_solver* s, int l, bool need_coarser = false) {
 
 // 3-D strided copy between a reference-layout host array and a pitched device buffer,
 // shape points only.
+// Fields of at least kStageMinBytes cross PCIe as one DMA of the host array's layout: a
+// device staging copy of that layout is filled by one contiguous copy (upload) or by the
+// repack kernel (download), so the link sees long contiguous runs instead of one short row
+// per (i, j); the repack between layouts runs at HBM speed.  The staging buffer is
+// allocated on first use and kept with the solver.
+constexpr size_t kStageMinBytes = 8u << 20;
+
+template <typename T>
+int repack_t(mgp_solver* s, int l, void* dev, bool to_device) {
+    LevelState& L = s->lv[l];
+    const mgp_level_info& I = L.info;
+    const long long off = I.halo[1] * I.stride[0] + I.halo[3] * I.stride[1] + I.halo[5];
+    const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
+    if (to_device)
+        return launch_k(s, k_repack<T, true>, dim3(grid_1d(s, n)), dim3(kThreads), 0, (T*)dev, L.G, (T*)s->stage, off,
+                        (long long)I.stride[0], (long long)I.stride[1]);
+    return launch_k(s, k_repack<T, false>, dim3(grid_1d(s, n)), dim3(kThreads), 0, (T*)dev, L.G, (T*)s->stage, off,
+                    (long long)I.stride[0], (long long)I.stride[1]);
+}
+
+int copy_field_staged(mgp_solver* s, int l, void* dev, void* host, bool to_device) {
+    LevelState& L = s->lv[l];
+    const mgp_level_info& I = L.info;
+    const size_t es = s->esize;
+    const size_t bytes = (size_t)I.size * es;
+    if (s->stage_bytes < bytes) {
+        if (s->stage) cudaFree(s->stage);
+        s->stage = nullptr;
+        s->stage_bytes = 0;
+        CK(cudaMalloc(&s->stage, bytes));
+        s->stage_bytes = bytes;
+    }
+    if (to_device) {
+        CK(cudaMemcpyAsync(s->stage, host, bytes, cudaMemcpyHostToDevice, s->stream));
+        CKS(DISPATCH(s, (repack_t<T>(s, l, dev, true))));
+    } else {
+        CKS(DISPATCH(s, (repack_t<T>(s, l, dev, false))));
+        // copy the shape points back with the longest contiguous runs the host layout has:
+        // k rows, whole (j, k) planes when z has no halo, the whole block when y has none too
+        const size_t off = (size_t)(I.halo[1] * I.stride[0] + I.halo[3] * I.stride[1] + I.halo[5]) * es;
+        size_t width = (size_t)L.G.nz * es, rows = (size_t)L.G.ny, planes = (size_t)L.G.nx;
+        size_t row_pitch = (size_t)I.stride[1] * es, plane_pitch = (size_t)I.stride[0] * es;
+        if (row_pitch == width) {
+            width *= rows;
+            rows = planes;
+            row_pitch = plane_pitch;
+            planes = 1;
+            if (row_pitch == width) {
+                width *= rows;
+                rows = 1;
+                row_pitch = width;
+            }
+        }
+        char* hb = (char*)host + off;
+        const char* sb = (const char*)s->stage + off;
+        if (planes == 1) {
+            CK(cudaMemcpy2DAsync(hb, row_pitch, sb, row_pitch, width, rows, cudaMemcpyDeviceToHost, s->stream));
+        } else {
+            cudaMemcpy3DParms p = {};
+            p.srcPtr = make_cudaPitchedPtr(const_cast<char*>(sb), row_pitch, width, (size_t)I.pad[1]);
+            p.dstPtr = make_cudaPitchedPtr(hb, row_pitch, width, (size_t)I.pad[1]);
+            p.extent = make_cudaExtent(width, rows, planes);
+            p.kind = cudaMemcpyDeviceToHost;
+            CK(cudaMemcpy3DAsync(&p, s->stream));
+        }
+    }
+    CK(cudaStreamSynchronize(s->stream));
+    return MGP_OK;
+}
+
 int copy_field(mgp_solver* s, int l, void* dev, void* host, bool to_device) {
     LevelState& L = s->lv[l];
     const mgp_level_info& I = L.info;
     const size_t es = s->esize;
+    if ((size_t)I.size * es >= kStageMinBytes) return copy_field_staged(s, l, dev, host, to_device);
     char* hbase = (char*)host + (size_t)(I.halo[1] * I.stride[0] + I.halo[3] * I.stride[1] + I.halo[5]) * es;
     cudaMemcpy3DParms p = {};
     cudaPitchedPtr hp = make_cudaPitchedPtr(hbase, (size_t)I.pad[2] * es, (size_t)L.G.nz * es, (size_t)I.pad[1]);
@@ -694,6 +767,7 @@ void release(mgp_solver* s) {
     }
     if (s->d_norm) cudaFree(s->d_norm);
     if (s->h_norm) cudaFreeHost(s->h_norm);
+    if (s->stage) cudaFree(s->stage);
     if (s->inner) release(s->inner);
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;

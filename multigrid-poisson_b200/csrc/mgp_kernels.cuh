@@ -1200,6 +1200,24 @@ __global__ void __launch_bounds__(256) k_fill_uniform(double* f, Geom G, unsigne
 }
 
 // Dirichlet::write_to (include/dirichlet.h:50-93): one face into its boundary plane.
+// Repacking between the pitched device layout and a device copy of the reference's
+// halo-padded host layout (stage[off + i*hs0 + j*hs1 + k]); only shape points move, so the
+// halo entries of the staging copy are neither read (TO_DEV) nor written (!TO_DEV).
+template <typename T, bool TO_DEV>
+__global__ void __launch_bounds__(256) k_repack(T* dev, Geom G, T* stage, long long off, long long hs0, long long hs1) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.nz);
+        const long long q = t / G.nz;
+        const int j = (int)(q % G.ny);
+        const int i = (int)(q / G.ny);
+        const long long pd = (long long)i * G.sx + (long long)j * G.sy + k;
+        const long long ph = off + i * hs0 + j * hs1 + k;
+        if (TO_DEV) dev[pd] = stage[ph];
+        else stage[ph] = dev[pd];
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_write_face(T* u, Geom G, const T* __restrict__ g, int fc) {
     int n0, n1;  // face extents in its two free dimensions
