@@ -71,6 +71,8 @@ typedef enum { MGP_CYCLE_RELAXATION = 0, MGP_CYCLE_V = 1, MGP_CYCLE_F = 2 } mgp_
                                  reference's resolution to Dirichlet (include/domain.h:140-145,191-192) */
 #define MGP_FLAG_REFINE_F32 16u /* iterative refinement, FP32 correction hierarchy (see mgp_solve) */
 #define MGP_FLAG_REFINE_F64 32u /* iterative refinement, FP64 correction hierarchy */
+#define MGP_FLAG_TMA_SWEEPS 64u /* levels of >= 2^20 points sweep with the TMA-fed kernel (shared-memory plane
+                                  rings filled by cp.async.bulk.tensor) instead of the per-thread cp.async march */
 #define MGP_FLAG_FUSED_SETUP 8u /* cycles form the residual inside the restriction kernel (one
                                    launch, r never stored) instead of residual + restriction */
 

@@ -28,6 +28,7 @@
 
 #include "mgp.h"
 #include "mgp_kernels.cuh"
+#include "mgp_stencil_tma.cuh"
 
 using namespace mgp;
 
@@ -86,6 +87,11 @@ struct LevelState {
     int cur = 0;            // index of the buffer that is "u" (Domain::swap_u, domain.h:311-316)
     bool gs_column = false; // padded y extent even: colour depends on (j,k) only; whole columns
     mgp_level_info info;    // host (reference) layout
+    // TMA-fed stencil sweeps (large levels): tensor maps of both u buffers and of f
+    bool tma = false;
+    CUtensorMap map_u[2];
+    CUtensorMap map_f;
+    TmaTiling tiling;
 };
 
 struct GraphEntry {
@@ -106,6 +112,7 @@ struct mgp_solver {
     std::vector<LevelState> lv;
     unsigned long long* d_norm = nullptr;  // [0] scratch for max-norms
     unsigned long long* h_norm = nullptr;  // pinned read-back
+    int* err_word = nullptr;               // kernels' wait-timeout flag (8 bytes after a norm word)
     void* stage = nullptr;                 // device copy of a host-layout field (large transfers)
     size_t stage_bytes = 0;
     std::map<std::tuple<int, int64_t, uint64_t, uint64_t>, GraphEntry> graphs;
@@ -189,6 +196,20 @@ int launch_k(mgp_solver* s, void (*kernel)(KArgs...), dim3 grid, dim3 block, siz
     return check_launch(s);
 }
 
+// Ordinary stream-ordered launch (the kernel starts after everything before it completed).
+template <typename... KArgs, typename... Act>
+int launch_k_ordered(mgp_solver* s, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, Act&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s->stream;
+    cfg.numAttrs = 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...);
+    if (e != cudaSuccess) return fail(MGP_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+    return check_launch(s);
+}
+
 // Blocks of `kernel` resident per SM (256 threads, static shared memory only).
 template <typename K>
 int resident_blocks(K kernel) {
@@ -232,6 +253,111 @@ void hsq_terms(T hsq, T& inv, int& pow2) {
     if (pow2 && !std::isnormal((double)inv)) pow2 = 0;
 }
 
+// ---- TMA-fed sweeps ------------------------------------------------------------------------
+// With MGP_FLAG_TMA_SWEEPS, levels of at least kTmaMinPoints points (and at least 3 points per
+// axis) sweep with k_stencil_tma.  Off by default: on B200 the per-thread cp.async march of
+// k_stencil is faster (513x257x129 FP64 Jacobi sweep 85 us against 128-140 us).
+constexpr long long kTmaMinPoints = 1ll << 20;
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiledFn) nullptr;
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
+// A 3-D map (k, j, i) of one pitched field buffer with a (box_k, box_j, 1) box; reads outside
+// the level's shape are filled with zeros.
+bool encode_field_map(CUtensorMap* m, void* base, bool f64, const Geom& G, int box_k, int box_j) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint64_t es = f64 ? 8 : 4;
+    const cuuint64_t dims[3] = {(cuuint64_t)G.nz, (cuuint64_t)G.ny, (cuuint64_t)G.nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)G.sy * es, (cuuint64_t)G.sx * es};
+    const cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_j, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tiles of kTmaTJ rows x BK points: BK is the largest multiple of V and HK that keeps a u box
+// within 256 elements and a CTA within kTmaMaxThreads threads, evened out over the k tiles.
+template <typename T>
+TmaTiling tma_tiling(const Geom& G) {
+    constexpr int V = VecT<T>::V, HK = tma_hk<T>(), Q = V > HK ? V : HK;
+    int bkmax = std::min(256 - 2 * HK, (kTmaMaxThreads / kTmaTJ) * V) / Q * Q;
+    TmaTiling t;
+    t.ntk = (G.nz + bkmax - 1) / bkmax;
+    t.BK = ((G.nz + t.ntk - 1) / t.ntk + Q - 1) / Q * Q;
+    t.ntj = (G.ny + kTmaTJ - 1) / kTmaTJ;
+    t.nvec = t.BK / V;
+    t.slot_u = (int)(((size_t)(kTmaTJ + 2) * (t.BK + 2 * HK) * sizeof(T) + 127) / 128 * 128);
+    t.slot_f = (int)(((size_t)kTmaTJ * t.BK * sizeof(T) + 127) / 128 * 128);
+    t.work = (long long)t.ntj * t.ntk * G.nx;
+    t.whole_tiles = 0;
+    return t;
+}
+
+template <typename T>
+size_t tma_smem(const TmaTiling& t) {
+    return (size_t)kTmaRingU * t.slot_u + (size_t)kTmaRingF * t.slot_f + 128;
+}
+
+template <typename T>
+void tma_prepare_level(mgp_solver* s, LevelState& L) {
+    L.tma = false;
+    const Geom& G = L.G;
+    if (!(s->desc.flags & MGP_FLAG_TMA_SWEEPS) || (long long)G.nx * G.ny * G.nz < kTmaMinPoints || G.nx < 3 ||
+        G.ny < 3 || G.nz < 3)
+        return;
+    constexpr int HK = tma_hk<T>();
+    L.tiling = tma_tiling<T>(G);
+    const bool f64 = sizeof(T) == 8;
+    const int bu = L.tiling.BK + 2 * HK, bf = L.tiling.BK;
+    bool ok = encode_field_map(&L.map_u[0], L.ubuf[0], f64, G, bu, kTmaTJ + 2) &&
+              encode_field_map(&L.map_f, L.f, f64, G, bf, kTmaTJ);
+    if (ok && L.ubuf[1]) ok = encode_field_map(&L.map_u[1], L.ubuf[1], f64, G, bu, kTmaTJ + 2);
+    else L.map_u[1] = L.map_u[0];
+    L.tma = ok;
+}
+
+// Launch of k_stencil_tma; src must be one of the level's u buffers.
+template <typename T, int OP, bool NORM>
+int launch_stencil_tma(mgp_solver* s, int l, const StencilArgs<T>& a) {
+    LevelState& L = s->lv[l];
+    const CUtensorMap& mu = a.src == L.ubuf[0] ? L.map_u[0] : L.map_u[1];
+    TmaTiling t = L.tiling;
+    const size_t smem = tma_smem<T>(t);
+    auto kernel = k_stencil_tma<T, OP, NORM>;
+    static bool attr_set[64] = {};  // per instantiation and device
+    if (s->device < 64 && !attr_set[s->device]) {
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_set[s->device] = true;
+    }
+    const int threads = kTmaTJ * t.nvec;
+    int grid;
+    if (OP == OP_GS_COLUMN) {
+        t.whole_tiles = 1;
+        grid = t.ntj * t.ntk;
+    } else {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        grid = (int)std::min<long long>(t.work, (long long)sm_count(s->device) * per_sm);
+    }
+    return launch_k_ordered(s, kernel, dim3(grid), dim3(threads), smem, mu, L.map_f, a, t, s->err_word);
+}
+
 // ---- stencil launches -------------------------------------------------------------------
 template <typename T, int OP>
 int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, int colour, unsigned long long* norm) {
@@ -251,6 +377,10 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
     a.colour = colour;
     a.norm = norm;
+    if (L.tma && (src == L.ubuf[0] || src == L.ubuf[1])) {
+        if (OP == OP_RESIDUAL && norm) return launch_stencil_tma<T, OP, true>(s, l, a);
+        return launch_stencil_tma<T, OP, false>(s, l, a);
+    }
     constexpr int V = VecT<T>::V;
     const int plane = L.G.ny * ((L.G.nz + V - 1) / V);  // threads per plane
     const int bx = (plane + kThreads - 1) / kThreads;
@@ -541,8 +671,14 @@ int launch_iteration(mgp_solver* s, int cycle, int64_t ns, double omega) {
 }
 
 int read_norm(mgp_solver* s, double* out) {
-    CK(cudaMemcpyAsync(s->h_norm, s->d_norm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->stream));
+    // the norm word and, 8 bytes on, the error word of the TMA-fed sweeps
+    CK(cudaMemcpyAsync(s->h_norm, s->d_norm, 16, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
+    if (reinterpret_cast<const int*>(s->h_norm)[2]) {
+        CK(cudaMemsetAsync(s->err_word, 0, sizeof(int), s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        return fail(MGP_ERR_TIMEOUT, "stencil sweep: a shared-memory ring wait ran out of time; results are invalid");
+    }
     double v;
     unsigned long long b = *s->h_norm;
     memcpy(&v, &b, sizeof(v));
@@ -960,9 +1096,15 @@ static int create_plain(const mgp_desc* d, mgp_solver** out) {
     }
     for (int l = 0; l < s->levels; l++)
         s->lv[l].G.poff = s->lv[l].gs_column ? (int)((hs + hb) & 1) : (int)((hw + hs + hb) & 1);
+    for (int l = 0; l < s->levels; l++) {
+        if (s->dtype == MGP_F64) tma_prepare_level<double>(s, s->lv[l]);
+        else tma_prepare_level<float>(s, s->lv[l]);
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_norm, 64);
+    if (e == cudaSuccess) e = cudaMemset(s->d_norm, 0, 64);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_norm, 64);
+    s->err_word = reinterpret_cast<int*>(reinterpret_cast<char*>(s->d_norm) + 8);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         release(s);
@@ -1001,6 +1143,7 @@ int mgp_create(const mgp_desc* d, mgp_solver** out) {
     cudaStreamDestroy(inner->stream);
     inner->stream = outer->stream;
     inner->owns_stream = false;
+    inner->err_word = outer->err_word;  // seen by the outer solver's norm read-back
     outer->inner = inner;
     outer->desc = *d;  // keeps the refine flag and the user's level count
     *out = outer;

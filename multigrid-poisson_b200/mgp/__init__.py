@@ -39,6 +39,7 @@ FLAG_STRICT_BC = 1
 FLAG_FUSED_SETUP = 8
 FLAG_REFINE_F32 = 16
 FLAG_REFINE_F64 = 32
+FLAG_TMA_SWEEPS = 64
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,
