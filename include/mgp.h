@@ -74,7 +74,8 @@ typedef enum { MGP_CYCLE_RELAXATION = 0, MGP_CYCLE_V = 1, MGP_CYCLE_F = 2 } mgp_
 #define MGP_FLAG_TMA_SWEEPS 64u /* levels of >= 2^20 points sweep with the TMA-fed kernel (shared-memory plane
                                   rings filled by cp.async.bulk.tensor) instead of the per-thread cp.async march */
 #define MGP_FLAG_FUSED_SETUP 8u /* cycles form the residual inside the restriction kernel (one
-                                   launch, r never stored) instead of residual + restriction */
+                                   launch, r never stored) on every level; without the flag only
+                                   levels of at most 2^20 points do */
 
 /* Settings (include/settings.h:14-39) plus the BoundaryCondition and the template choice. */
 typedef struct mgp_desc {

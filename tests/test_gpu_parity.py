@@ -150,6 +150,30 @@ def test_cycle_bit_exact(mgp_mod, gpu_ready, ci, cycle):
             assert_face_equal(o, e, fc, l)
 
 
+FUSED_LARGE = [
+    # coarse levels wider than one k tile of the fused kernel (31 coarse points) and taller
+    # than one j tile
+    ((33, 33, 129), 3, (1, 1, 1, 1, 0, 0), "fw", "jacobi"),
+    ((65, 17, 97), 3, (0, 0, 1, 1, 1, 1), "fw", "gs"),
+    ((33, 65, 65), 3, (0, 0, 1, 1, 1, 1), "inj", "gs"),
+]
+
+
+@pytest.mark.parametrize("ci", range(len(FUSED_LARGE)))
+def test_fused_setup_large_bit_exact(mgp_mod, gpu_ready, ci):
+    cfg = cfg_of(FUSED_LARGE[ci], h=1.0 / 128)
+    o = make_oracle(cfg)
+    randomize(o, 90 + ci)
+    e = make_engine(mgp_mod, cfg, flags=mgp_mod.FLAG_FUSED_SETUP)
+    push(o, e)
+    om = o.default_omega()
+    o.fcycle(0, om, 2)
+    e.fcycle(0, om, 2)
+    for l in range(o.levels):
+        assert_field_equal(o, e, "u", l)
+        assert_field_equal(o, e, "f", l)
+
+
 @pytest.mark.parametrize("ci", range(len(CONFIGS)))
 def test_fused_setup_cycle_bit_exact(mgp_mod, gpu_ready, ci):
     """The one-kernel residual+restriction form of the coarse-grid set-up."""
