@@ -136,7 +136,9 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str | None = None):
+    """One process per GPU under torchrun: (world, rank, local_rank, process group or None).
+    NCCL on GPU boxes; gloo where no GPU is visible (the host-side tests of the N>1 path)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -147,8 +149,12 @@ def dist_setup(n_gpus: int):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if not dist.is_initialized():
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -159,13 +165,21 @@ def barrier(pg):
 
 
 def max_over_ranks(pg, x: float, local: int) -> float:
+    """The largest x over all ranks (times are taken as the slowest rank's)."""
     if pg is None:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput: every rank processed units_per_rank; the job took the slowest
+    rank's time (weak scaling: replicas of the same workload)."""
+    return units_per_rank * world / seconds_max
 
 
 def build_solver(mgp, device: int, maxiter: int, pinned: bool):
@@ -482,7 +496,7 @@ def main():
     sec = ev0.elapsed_time(ev1) / 1e3
     assert st.cycles_run == args.steps, (st.cycles_run, args.steps)
     tmax = max_over_ranks(pg, sec, local)
-    value = NDOF * args.steps * world / tmax
+    value = aggregate(NDOF * args.steps, world, tmax)
 
     # e2e through the reference-facing API: to_device + solve(4 F-cycles) + to_host per request
     eng.set_iteration_limits(E2E_CYCLES, E2E_CYCLES, 0.0)
@@ -502,7 +516,7 @@ def main():
     e1.synchronize()
     barrier(pg)
     e2e_sec = max_over_ranks(pg, e0.elapsed_time(e1) / 1e3 / n_e2e, local)
-    e2e_value = NDOF * E2E_CYCLES * world / e2e_sec
+    e2e_value = aggregate(NDOF * E2E_CYCLES, world, e2e_sec)
     esz = 8
     lv = ps.engine.level[0]
     face_elems = sum(a * b * c for a, b, c in lv.face_shape)
