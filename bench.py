@@ -45,6 +45,8 @@ H = 1.0 / 512
 BC = (1, 1, 1, 1, 0, 0)  # N S E W T B requested
 NSMOOTH = 2
 E2E_CYCLES = 4
+REF_ARM_CYCLES = 30   # timed cycles of the reference arm (a bounded sample)
+CPU_BASELINE_CYCLES = 8
 NDOF = DIMS[0] * DIMS[1] * DIMS[2]
 METRIC = "F-cycle fine-grid DOF/s (FP64, 513x257x129)"
 UNIT = "DOF*cycles/s"
@@ -433,7 +435,11 @@ def run_reference_arm(args):
     if not REF_BIN.exists():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref/ref_oracle not built"}))
         return 0
-    res = cpu_reference(args.steps, args.warmup)
+    # Bounded sample: the reference takes ~1 s per F-cycle of this grid on 16 host threads, so
+    # at most REF_ARM_CYCLES timed cycles (after at most 2 warm-up cycles) keep the run to a
+    # minute or so whatever --steps says; the metric is per cycle, so the sample size does not
+    # change it.
+    res = cpu_reference(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2))
     cores = res["threads"]
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(1, res["cycles"]),
@@ -535,7 +541,7 @@ def main():
     cpu = None
     if not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference(steps=2, warm=0)
+            cpu = cpu_reference(steps=CPU_BASELINE_CYCLES, warm=0)
         except Exception as exc:  # noqa: BLE001 -- the baseline is informative only
             cpu = {"error": str(exc)}
     clocks = clk.summary()
