@@ -550,19 +550,44 @@ int coarse_setup_fused_t(mgp_solver* s, int l) {
     a.hsq = (T)(F.h * F.h);
     hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
     a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
-    // coarse tile: tkc points along k (2*tkc a multiple of V keeps rows aligned), tjc rows
-    int tkc = V == 2 ? 31 : 30;
-    if (C.G.nz < tkc) tkc = (V == 2) ? C.G.nz : (C.G.nz + 1) / 2 * 2;
-    const int tkv = (2 * tkc + V) / V;
-    const int tjc = std::max(1, std::min(C.G.ny, (256 / tkv - 1) / 2));
+    // Coarse tile: tkc points along k (balanced over the k tiles of a row; 2*tkc a multiple of
+    // V keeps the fine rows' vectors aligned) by tjc rows, chosen for the fewest idle lanes
+    // per coarse point in blocks of at most 384 threads (two blocks per SM).
+    const int kmax = V == 2 ? 31 : 30;
+    const int ntk = (C.G.nz + kmax - 1) / kmax;
+    int tkc = (C.G.nz + ntk - 1) / ntk;
+    tkc = (2 * tkc + V - 1) / V * V / 2;
+    const int tkv = 2 * tkc / V + 1;
+    int tjc = 1;
+    double best = 1e30;
+    for (int c = 1; c <= std::min(C.G.ny, 16); c++) {
+        const int thr = tkv * (2 * c + 1);
+        if (thr > 384) break;
+        const double cost = (double)((thr + 31) / 32 * 32) / (double)(c * std::min(tkc, C.G.nz));
+        if (cost < best - 1e-9) {
+            best = cost;
+            tjc = c;
+        }
+    }
     const int rows = 2 * tjc + 1;
     a.tkc = tkc;
     a.tjc = tjc;
     a.tiles_j = (C.G.ny + tjc - 1) / tjc;
     a.tiles_k = (C.G.nz + tkc - 1) / tkc;
     const int tiles = a.tiles_j * a.tiles_k;
-    const int target = sm_count(s->device) * 8;
-    const int chunks = std::max(1, std::min((target + tiles - 1) / tiles, C.G.nx));
+    const size_t smem = rr_smem_bytes<T>(tkv, rows);
+    static bool attr_set[2][64] = {};  // per dtype and device
+    bool& set = attr_set[sizeof(T) == 8][s->device & 63];
+    if (!set) {
+        // the largest block (384 threads) needs less than 160 KB
+        CK(cudaFuncSetAttribute(k_resid_restrict<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        set = true;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resid_restrict<T>, tkv * rows, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int chunks = march_chunks(tiles, C.G.nx, sm_count(s->device) * per_sm);
     a.ci = (C.G.nx + chunks - 1) / chunks;
     const int nchunks = (C.G.nx + a.ci - 1) / a.ci;
     a.main_blocks = tiles * nchunks;
@@ -577,7 +602,6 @@ int coarse_setup_fused_t(mgp_solver* s, int l) {
         a.bc_blocks_per_face = (int)std::max(1ll, std::min(64ll, (nmax + tkv * rows - 1) / (tkv * rows)));
         extra = 6 * a.bc_blocks_per_face;
     }
-    const size_t smem = (size_t)3 * rows * (tkv * V) * sizeof(T);
     return launch_k(s, k_resid_restrict<T>, dim3(a.main_blocks + extra), dim3(tkv, rows), smem, a);
 }
 

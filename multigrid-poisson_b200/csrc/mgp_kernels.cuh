@@ -221,14 +221,15 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
         const int i1 = inr ? min(ib, G.x1) : i0;
         if (NORM) {
             // r outside the bounds keeps its value and still counts in the norm
-            // (infinity_norm runs over the whole shape, devicearray.h:221-237).
+            // (infinity_norm runs over the whole shape, devicearray.h:221-237).  Here: the
+            // planes of the chunk outside the i bounds (all of them when this vector has no
+            // relaxed point); the unrelaxed points of relaxed planes are read in the march.
             for (int i = ia; i < ib; i++) {
-                const unsigned m = (i >= i0 && i < i1) ? (ins & ~inr) : ins;
-                if (!m) continue;
+                if (i >= i0 && i < i1) continue;
                 const T* rp = a.dst + (long long)i * G.sx + bjk;
 #pragma unroll
                 for (int e = 0; e < V; e++)
-                    if ((m >> e) & 1u) mx = max(mx, abs_bits(rp[e]));
+                    if ((ins >> e) & 1u) mx = max(mx, abs_bits(rp[e]));
             }
         }
         if (i0 < i1) {
@@ -291,6 +292,12 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
 #pragma unroll
                     for (int e = 0; e < V; e++)
                         if (((base + e) & 1) != a.colour) act &= ~(1u << e);
+                }
+                if (NORM && (ins & ~inr)) {  // stored r at the unrelaxed points of this plane
+                    const T* rp = a.dst + p;
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if (((ins & ~inr) >> e) & 1u) mx = max(mx, abs_bits(rp[e]));
                 }
                 T cur[V];
 #pragma unroll
@@ -505,15 +512,29 @@ __global__ void __launch_bounds__(256) k_restrict_bc(BcRestrictArgs<T> a) {
 
 // ------------------------------------------------------------------------------------
 // Coarse-grid set-up in one pass (include/vcycle.h:34-76): the residual of level l is
-// formed plane by plane and never stored; each block keeps the last three residual planes
-// of its (j,k) tile in shared memory and, every second plane, restricts them into f_{l+1}
-// (Injection or FullWeighting, the reference's summation order) and zeroes u_{l+1}.
-// Blocks past `main_blocks` restrict the Neumann face data instead.
+// formed plane by plane and never stored, restricted into f_{l+1} (Injection or
+// FullWeighting), and u_{l+1} is zeroed.  Blocks past `main_blocks` restrict the Neumann
+// face data instead.
 //
-// Block = (tkv, 2*tjc+1) threads: one thread per fine (row, k-vector) of the tile.  The
-// tile covers fine rows 2*J0-1 .. 2*(J0+tjc)-1 and fine k from 2*K0-V, so every fine point a
-// coarse point of the tile reads is inside it.  Residual values at points outside the
-// relaxation bounds are the stored r (the reference restricts whatever r holds there).
+// FullWeighting's coarse value is (((T)s_m + s_0) + s_p) / 64, each s a left-to-right sum
+// over the fine planes im, ii, ip in that order (include/fullweighting.h:82-114).  A march
+// in increasing i meets those planes in the same order, so every coarse point of the block
+// carries its three partial sums in registers from one fine plane to the next and only one
+// fine plane's residual tile lives in shared memory.  Fine plane i adds to coarse plane
+// (i+1)/2 as im (odd i), i/2 as ii (even i) and (i-1)/2 as ip (odd i); the clamped first and
+// last planes also act as im of plane 0 and as ip of the last plane.
+//
+// Block = (tkv, 2*tjc+1) threads: one thread per fine (row, k-vector) of the tile, which
+// covers fine rows 2*J0-1 .. 2*(J0+tjc)-1 and fine k from 2*K0-V, so every fine point a
+// coarse point of the tile reads is inside it; the first tjc*tkc threads also own one coarse
+// point each.  Everything a plane needs is staged by cp.async kRingU-2 planes ahead into a
+// ring of shared-memory slots: the u plane tile with one halo row and column on each side
+// (each thread copies its own vector, the edge threads the halo), each thread's f vector
+// (its stored r on planes outside the relaxation bounds), and, for the threads on the
+// boundary rows and columns of the shape, the stored r of their unrelaxed points and the
+// Neumann face values of their ghosts.  One barrier per plane: after it, the plane's data
+// have landed, the slot of the plane before it is free for the next copy, and the previous
+// plane's residual tile is complete for the coarse points to read.
 template <typename T>
 struct RRArgs {
     Geom Gf, Gc;
@@ -531,8 +552,94 @@ struct RRArgs {
     BcRestrictArgs<T> bc;
 };
 
+// The share of fine plane q (residual tile P, rows pre-multiplied by the tile row width) in
+// the coarse point's restriction: Injection at the coarse plane q/2, or FullWeighting's
+// running sums, i-major with weights (1,2,1 | 2,4,2 | 1,2,1), doubled on the ii plane.
 template <typename T>
-__global__ void __launch_bounds__(512) k_resid_restrict(RRArgs<T> a) {
+__device__ __forceinline__ void rr_accumulate(const T* P, int q, const RRArgs<T>& a, int I0, int I1, int nxf, int rm,
+                                              int rj, int rp, int cm, int ck, int cp, long long o, double& s_m,
+                                              double& s_0, double& s_p) {
+    const Geom& Gc = a.Gc;
+    if (!a.fw) {
+        if (!(q & 1) && (q >> 1) >= I0 && (q >> 1) < I1) {  // injection.h:63
+            const long long oo = (long long)(q >> 1) * Gc.sx + o;
+            a.fc[oo] = P[rj + ck];
+            a.uc[oo] = T(0);
+        }
+        return;
+    }
+    auto A = [&](int row, int col) -> double { return (double)P[row + col]; };
+    // w = 1 on the im and ip planes, 2 on the ii plane; `first` starts the sums
+    auto add = [&](double w, bool first) {
+        if (first) {
+            s_m = w * A(rm, cm);
+            s_0 = (2.0 * w) * A(rm, ck);
+            s_p = w * A(rm, cp);
+        } else {
+            s_m = s_m + w * A(rm, cm);
+            s_0 = s_0 + (2.0 * w) * A(rm, ck);
+            s_p = s_p + w * A(rm, cp);
+        }
+        s_m = s_m + (2.0 * w) * A(rj, cm);
+        s_m = s_m + w * A(rp, cm);
+        s_0 = s_0 + (4.0 * w) * A(rj, ck);
+        s_0 = s_0 + (2.0 * w) * A(rp, ck);
+        s_p = s_p + (2.0 * w) * A(rj, cp);
+        s_p = s_p + w * A(rp, cp);
+    };
+    auto finish = [&](int I) {  // (((T)s_m + s_0) + s_p) / 64
+        T tmp = (T)s_m;
+        tmp = (T)((double)tmp + s_0);
+        tmp = (T)((double)tmp + s_p);
+        const long long oo = (long long)I * Gc.sx + o;
+        a.fc[oo] = (T)((double)tmp / 64.0);
+        a.uc[oo] = T(0);
+    };
+    if (q & 1) {
+        const int Ip = (q - 1) >> 1, Im = (q + 1) >> 1;
+        if (Ip >= I0 && Ip < I1) {
+            add(1.0, false);
+            finish(Ip);
+        }
+        if (Im >= I0 && Im < I1) add(1.0, true);
+    } else {
+        const int Ic = q >> 1;
+        if (Ic >= I0 && Ic < I1) {
+            if (q == 0) add(1.0, true);
+            add(2.0, false);
+            if (q == nxf - 1) {
+                add(1.0, false);
+                finish(Ic);
+            }
+        }
+    }
+}
+
+constexpr int kRingU = 5;  // ring depth of k_resid_restrict (planes i, i+1 in use, 3 in flight)
+
+// Shared memory of k_resid_restrict for a (tkv, rows) block: u tiles, f slots and boundary
+// slots per ring stage, then two residual plane tiles.
+template <typename T>
+constexpr size_t rr_smem_bytes(int tkv, int rows) {
+    return ((size_t)kRingU * ((rows + 2) * (tkv + 2) + tkv * rows + 2 * (2 * tkv + 2 * rows)) * VecT<T>::V +
+            (size_t)2 * rows * tkv * VecT<T>::V) *
+           sizeof(T);
+}
+
+// cp.async of one 4- or 8-byte element (the L1-allocating form is the only one below 16 bytes)
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"((int)sizeof(T)) : "memory");
+}
+// 16-byte cp.async that bypasses L1 (the block reads the data from shared memory only)
+__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(384, 2) k_resid_restrict(RRArgs<T> a) {
     pdl_begin();
     if ((int)blockIdx.x >= a.main_blocks) {
         const int b = blockIdx.x - a.main_blocks;
@@ -545,12 +652,21 @@ __global__ void __launch_bounds__(512) k_resid_restrict(RRArgs<T> a) {
         return;
     }
     constexpr int V = VecT<T>::V;
+    constexpr int SW = 2 * V;  // boundary slot: V values (stored r or S/N face), bottom and top face
     extern __shared__ __align__(16) unsigned char rr_smem[];
-    T* ring = reinterpret_cast<T*>(rr_smem);
     const Geom& Gf = a.Gf;
     const Geom& Gc = a.Gc;
-    const int TW = blockDim.x * V;
-    const int PE = blockDim.y * TW;  // elements of one residual plane tile
+    const int TKV = blockDim.x, R = blockDim.y;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int TW = TKV * V;       // elements of one residual tile row
+    const int US = TW + 2 * V;    // u tile row: V-1 pad, k halo, TW points, k halo, V-1 pad
+    const int nthr = TKV * R;
+    const int tid = ty * TKV + tx;
+    const int NB = 2 * TKV + 2 * R;  // boundary slots per stage
+    // one ring stage: u tile, f vectors, boundary slots
+    const int STG = (R + 2) * US + nthr * V + NB * SW;
+    T* ring = reinterpret_cast<T*>(rr_smem);
+    T* rtile = ring + kRingU * STG;
     int b = blockIdx.x;
     const int tj = b % a.tiles_j;
     b /= a.tiles_j;
@@ -559,8 +675,8 @@ __global__ void __launch_bounds__(512) k_resid_restrict(RRArgs<T> a) {
     const int J0 = tj * a.tjc, K0 = tk * a.tkc;
     const int I0 = chunk * a.ci, I1 = min(Gc.nx, I0 + a.ci);
     const int jf0 = 2 * J0 - 1, kf0 = 2 * K0 - V;
-    const int j = jf0 + (int)threadIdx.y;
-    const int kb = kf0 + (int)threadIdx.x * V;
+    const int j = jf0 + ty;
+    const int kb = kf0 + tx * V;
     unsigned ins = 0u, inr = 0u;
     const bool jok = j >= 0 && j < Gf.ny;
     const bool jin = j >= Gf.y0 && j < Gf.y1;
@@ -572,138 +688,182 @@ __global__ void __launch_bounds__(512) k_resid_restrict(RRArgs<T> a) {
             if (jin && k >= Gf.z0 && k < Gf.z1) inr |= 1u << e;
         }
     }
-    const long long bjk = (long long)j * Gf.sy + kb;  // used only when ins != 0
-    const int ia = max(0, 2 * I0 - 1), ib = min(Gf.nx - 1, 2 * I1 - 1);
+    const int ia = max(0, 2 * I0 - 1), ib = min(Gf.nx - 1, 2 * I1 - 1);  // fine planes ia..ib
+    const int pend = min(ib + 1, Gf.nx - 1);                              // last u plane read
+    // ---- this thread's copies, as (shared offset in a stage, global offset in a plane) ----
+    const long long g_own = (long long)j * Gf.sy + kb;
+    const int s_own = (ty + 1) * US + V + tx * V;
+    // halo row: the first and last rows of threads also copy the row beyond them
+    const int hrow = ty == 0 ? 0 : (ty == R - 1 ? R + 1 : -1);
+    const int jh = jf0 - 1 + hrow;
+    const bool c_hr = hrow >= 0 && jh >= 0 && jh < Gf.ny && kb >= 0 && kb < Gf.nz;
+    const long long g_hr = (long long)jh * Gf.sy + kb;
+    const int s_hr = hrow * US + V + tx * V;
+    // halo column: the first and last threads of a row copy the point beyond them
+    const int kh = tx == 0 ? kf0 - 1 : (tx == TKV - 1 ? kf0 + TW : -1);
+    const bool c_hc = (tx == 0 || tx == TKV - 1) && jok && kh >= 0 && kh < Gf.nz;
+    const long long g_hc = (long long)j * Gf.sy + kh;
+    const int s_hc = (ty + 1) * US + (tx == 0 ? V - 1 : V + TW);
+    const int s_f = (R + 2) * US + tid * V;
+    // boundary slot: rows 0 / ny-1 of the shape, then the vectors holding k = 0 / nz-1
+    const unsigned m_r = ins & ~inr;                                           // stored r
+    const unsigned m_sn = ((j == 0 || j == Gf.ny - 1) && jin) ? inr : 0u;      // S/N ghosts
+    const bool need_b = (inr & 1u) && kb == 0;                                 // bottom ghost
+    int e_top = Gf.nz - 1 - kb;
+    const bool need_t = e_top >= 0 && e_top < V && ((inr >> e_top) & 1u);    // top ghost
+    e_top = max(0, min(V - 1, e_top));
+    int bslot = -1;
+    if (j == 0) bslot = tx;
+    else if (j == Gf.ny - 1) bslot = TKV + tx;
+    else if (kb == 0) bslot = 2 * TKV + ty;
+    else if (kb <= Gf.nz - 1 && Gf.nz - 1 < kb + V) bslot = 2 * TKV + R + ty;
+    const bool c_bd = bslot >= 0 && (m_r || m_sn || need_b || need_t);
+    const int s_bd = (R + 2) * US + nthr * V + max(bslot, 0) * SW;
+    const T* g_sn = j == 0 ? a.F.g[F_SOUTH] : a.F.g[F_NORTH];
+    const T* u = a.u;
+    const T* f = a.f;
+    const T* r = a.r;
+    // copies of plane p into ring stage `st`
+    auto stage = [&](int p, int st) {
+        T* S = ring + st * STG;
+        if (p <= pend) {
+            const long long pp = (long long)p * Gf.sx;
+            if (ins) cp_async16_cg(S + s_own, u + pp + g_own);
+            if (c_hr) cp_async16_cg(S + s_hr, u + pp + g_hr);
+            if (c_hc) cp_async_elem(S + s_hc, u + pp + g_hc);
+            if (p <= ib) {
+                const bool inside = p >= Gf.x0 && p < Gf.x1;
+                if (ins) cp_async16_cg(S + s_f, (inside ? f : r) + pp + g_own);
+                if (c_bd && inside) {
+                    T* B = S + s_bd;
+#pragma unroll
+                    for (int e = 0; e < V; e++) {
+                        if ((m_r >> e) & 1u) cp_async_elem(B + e, r + pp + g_own + e);
+                        else if ((m_sn >> e) & 1u) cp_async_elem(B + e, g_sn + (long long)p * Gf.nz + kb + e);
+                    }
+                    if (need_b) cp_async_elem(B + V, a.F.g[F_BOTTOM] + (long long)p * Gf.ny + j);
+                    if (need_t) cp_async_elem(B + V + 1, a.F.g[F_TOP] + (long long)p * Gf.ny + j);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    int st_fill = 0;
+#pragma unroll 1
+    for (int q = 0; q < kRingU - 1; q++) {
+        stage(ia + q, st_fill);
+        st_fill++;
+    }
     const T two_h = a.two_h, m2h = -a.two_h;
-    T vm[V], vc[V], vp[V], vpp[V], fcur[V], fn[V], vmo[V];
+    T vm[V];  // this thread's u(i-1)
     if (ins) {
-        ldv(vc, a.u + (long long)ia * Gf.sx + bjk);
         if (ia > 0) {
-            ldv(vm, a.u + (long long)(ia - 1) * Gf.sx + bjk);
-        } else {
+            ldv(vm, u + (long long)(ia - 1) * Gf.sx + g_own);
+        } else {  // west ghost  -2h*gW + u(1)
             T v1[V];
-            ldv(v1, a.u + Gf.sx + bjk);
+            ldv(v1, u + Gf.sx + g_own);
 #pragma unroll
             for (int e = 0; e < V; e++)
                 vm[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_WEST] + (long long)j * Gf.nz + kb + e) + v1[e] : T(0);
         }
-#pragma unroll
-        for (int e = 0; e < V; e++) vmo[e] = vm[e];
-        if (ia + 1 < Gf.nx) ldv(vp, a.u + (long long)(ia + 1) * Gf.sx + bjk);
-        ldv(fcur, a.f + (long long)ia * Gf.sx + bjk);
     }
-    T* myslot = ring + threadIdx.y * TW + threadIdx.x * V;
+    // this thread's coarse point (J, K) and its 3x3 fine (row, column) neighbourhood in the tile
+    const int J = J0 + tid / a.tkc, K = K0 + tid % a.tkc;
+    const bool owner = tid < a.tjc * a.tkc && J < Gc.ny && K < Gc.nz;
+    const int rj = (2 * J - jf0) * TW, rm = (max(0, 2 * J - 1) - jf0) * TW, rp = (min(Gf.ny - 1, 2 * J + 1) - jf0) * TW;
+    const int ck = 2 * K - kf0, cm = max(0, 2 * K - 1) - kf0, cp = min(Gf.nz - 1, 2 * K + 1) - kf0;
+    const long long o = (long long)J * Gc.sy + K;
+    double s_m = 0.0, s_0 = 0.0, s_p = 0.0;
+    int st_cur = 0;  // ring stage of plane i
+#pragma unroll 1
     for (int i = ia; i <= ib; i++) {
-        const long long p = (long long)i * Gf.sx + bjk;
+        cp_async_wait<kRingU - 3>();  // this thread's copies of planes i and i+1 have landed
+        __syncthreads();
+        stage(i + kRingU - 1, st_fill);  // into the stage of plane i-1, which every thread is done with
+        st_fill = st_fill + 1 == kRingU ? 0 : st_fill + 1;
+        const int st_nxt = st_cur + 1 == kRingU ? 0 : st_cur + 1;
         if (ins) {
-            if (i < ib) {
-                if (i + 2 < Gf.nx) ldv(vpp, a.u + p + 2 * Gf.sx);
-                ldv(fn, a.f + p + Gf.sx);
-            }
-            if (i + 1 == Gf.nx) {
-#pragma unroll
-                for (int e = 0; e < V; e++)
-                    vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * Gf.nz + kb + e) + vmo[e]
-                                              : T(0);
-            }
-            const unsigned act = (i >= Gf.x0 && i < Gf.x1) ? inr : 0u;
+            const T* S = ring + st_cur * STG;
+            const T* tu = S + s_own;  // u(i) at (j, kb)
             T val[V];
-            if (ins & ~act) {
-#pragma unroll
-                for (int e = 0; e < V; e++)
-                    val[e] = (((ins & ~act) >> e) & 1u) ? ldg(a.r + p + e) : T(0);
-            }
-            if (act) {
-                T ym[V], yp[V];
-                if (j > 0) {
-                    ldv(ym, a.u + p - Gf.sy);
-                } else {
-                    T w[V];
-                    ldv(w, a.u + p + Gf.sy);
+            if (i >= Gf.x0 && i < Gf.x1) {
+                T vc[V], vp[V], fcur[V], bd[SW];
+                lds_v(vc, tu);
+                if (i + 1 < Gf.nx) {
+                    lds_v(vp, ring + st_nxt * STG + s_own);
+                } else {  // east ghost  2h*gE + u(nx-2)
 #pragma unroll
                     for (int e = 0; e < V; e++)
-                        ym[e] = ((ins >> e) & 1u) ? m2h * ldg(a.F.g[F_SOUTH] + (long long)i * Gf.nz + kb + e) + w[e] : T(0);
-                }
-                if (j < Gf.ny - 1) {
-                    ldv(yp, a.u + p + Gf.sy);
-                } else {
-                    T w[V];
-                    ldv(w, a.u + p - Gf.sy);
-#pragma unroll
-                    for (int e = 0; e < V; e++)
-                        yp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_NORTH] + (long long)i * Gf.nz + kb + e) + w[e]
+                        vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * Gf.nz + kb + e) + vm[e]
                                                   : T(0);
                 }
-                const T left = kb > 0 ? ldg(a.u + p - 1) : T(0);
-                const T right = kb + V < Gf.nz ? ldg(a.u + p + V) : T(0);
+                lds_v(fcur, S + s_f);
+                if (c_bd) {
+#pragma unroll
+                    for (int e = 0; e < SW; e++) bd[e] = S[s_bd + e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < SW; e++) bd[e] = T(0);
+                }
+                T ym[V], yp[V];
+                if (j > 0) {
+                    lds_v(ym, tu - US);
+                } else {  // south ghost  -2h*gS + u(j=1)
+                    T w[V];
+                    lds_v(w, tu + US);
+#pragma unroll
+                    for (int e = 0; e < V; e++) ym[e] = m2h * bd[e] + w[e];
+                }
+                if (j < Gf.ny - 1) {
+                    lds_v(yp, tu + US);
+                } else {  // north ghost  2h*gN + u(j=ny-2)
+                    T w[V];
+                    lds_v(w, tu - US);
+#pragma unroll
+                    for (int e = 0; e < V; e++) yp[e] = two_h * bd[e] + w[e];
+                }
+                const T left = kb > 0 ? tu[-1] : T(0);
+                const T right = kb + V < Gf.nz ? tu[V] : T(0);
 #pragma unroll
                 for (int e = 0; e < V; e++) {
-                    if (!((act >> e) & 1u)) continue;
+                    if ((m_r >> e) & 1u) {
+                        val[e] = bd[e];  // stored r
+                        continue;
+                    }
+                    if (!((inr >> e) & 1u)) {
+                        val[e] = T(0);
+                        continue;
+                    }
                     const int k = kb + e;
                     const T below = e > 0 ? vc[e - 1] : left;
                     const T above = e < V - 1 ? vc[e + 1] : right;
-                    const T zm = k > 0 ? below : m2h * ldg(a.F.g[F_BOTTOM] + (long long)i * Gf.ny + j) + vc[1];
-                    const T zp = k < Gf.nz - 1 ? above : two_h * ldg(a.F.g[F_TOP] + (long long)i * Gf.ny + j) + below;
+                    const T zm = k > 0 ? below : m2h * bd[V] + vc[1];                     // -2h*gB + u(1)
+                    const T zp = k < Gf.nz - 1 ? above : two_h * bd[V + 1] + below;       // 2h*gT + u(nz-2)
                     const T sum = vm[e] + vp[e] + ym[e] + yp[e] + zm + zp;
                     val[e] = residual_pt(fcur[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
                 }
-            }
-            T* dst = myslot + (i % 3) * PE;
 #pragma unroll
-            for (int e = 0; e < V; e++) dst[e] = val[e];
+                for (int e = 0; e < V; e++) vm[e] = vc[e];
+            } else {  // a plane outside the relaxation bounds: the stored r, staged in the f slot
+                lds_v(val, S + s_f);
+                T vc[V];
+                lds_v(vc, tu);
 #pragma unroll
-            for (int e = 0; e < V; e++) {
-                vmo[e] = vc[e];
-                vm[e] = vc[e];
-                vc[e] = vp[e];
-                vp[e] = vpp[e];
-                fcur[e] = fn[e];
+                for (int e = 0; e < V; e++) vm[e] = vc[e];
             }
+            stv(rtile + (i & 1) * (R * TW) + ty * TW + tx * V, val);
         }
-        __syncthreads();
-        int I = -1;
-        if (i & 1) I = (i - 1) >> 1;
-        else if (i == Gf.nx - 1) I = i >> 1;
-        if (I >= I0 && I < I1) {
-            const int ii = 2 * I, im = max(0, ii - 1), ip = min(Gf.nx - 1, ii + 1);
-            const T* Pm = ring + (im % 3) * PE;
-            const T* P0 = ring + (ii % 3) * PE;
-            const T* Pp = ring + (ip % 3) * PE;
-            const int nthr = blockDim.x * blockDim.y;
-            for (int c = threadIdx.y * blockDim.x + threadIdx.x; c < a.tjc * a.tkc; c += nthr) {
-                const int J = J0 + c / a.tkc, K = K0 + c % a.tkc;
-                if (J >= Gc.ny || K >= Gc.nz) continue;
-                const int jj = 2 * J, jm = max(0, jj - 1), jp = min(Gf.ny - 1, jj + 1);
-                const int kk = 2 * K, km = max(0, kk - 1), kp = min(Gf.nz - 1, kk + 1);
-                const int rj = jj - jf0, rm = jm - jf0, rp = jp - jf0;
-                const int ck = kk - kf0, cm = km - kf0, cp = kp - kf0;
-                T out;
-                if (a.fw) {
-                    // FullWeighting::restrict_to order (fullweighting.h:76-109), k offset outermost
-                    auto A = [&](const T* P, int row, int col) -> double { return (double)P[row * TW + col]; };
-                    const double s_m = 1.0 * A(Pm, rm, cm) + 2.0 * A(Pm, rj, cm) + 1.0 * A(Pm, rp, cm) +
-                                       2.0 * A(P0, rm, cm) + 4.0 * A(P0, rj, cm) + 2.0 * A(P0, rp, cm) +
-                                       1.0 * A(Pp, rm, cm) + 2.0 * A(Pp, rj, cm) + 1.0 * A(Pp, rp, cm);
-                    T tmp = (T)s_m;
-                    const double s_0 = 2.0 * A(Pm, rm, ck) + 4.0 * A(Pm, rj, ck) + 2.0 * A(Pm, rp, ck) +
-                                       4.0 * A(P0, rm, ck) + 8.0 * A(P0, rj, ck) + 4.0 * A(P0, rp, ck) +
-                                       2.0 * A(Pp, rm, ck) + 4.0 * A(Pp, rj, ck) + 2.0 * A(Pp, rp, ck);
-                    tmp = (T)((double)tmp + s_0);
-                    const double s_p = 1.0 * A(Pm, rm, cp) + 2.0 * A(Pm, rj, cp) + 1.0 * A(Pm, rp, cp) +
-                                       2.0 * A(P0, rm, cp) + 4.0 * A(P0, rj, cp) + 2.0 * A(P0, rp, cp) +
-                                       1.0 * A(Pp, rm, cp) + 2.0 * A(Pp, rj, cp) + 1.0 * A(Pp, rp, cp);
-                    tmp = (T)((double)tmp + s_p);
-                    out = (T)((double)tmp / 64.0);
-                } else {
-                    out = P0[rj * TW + ck];  // injection.h:63
-                }
-                const long long o = (long long)I * Gc.sx + (long long)J * Gc.sy + K;
-                a.fc[o] = out;
-                a.uc[o] = T(0);
-            }
+        st_cur = st_nxt;
+        if (owner && i > ia) {
+            // the coarse points' share of fine plane i-1, whose residual tile is complete
+            const int q = i - 1;
+            const T* P = rtile + (q & 1) * (R * TW);
+            rr_accumulate(P, q, a, I0, I1, Gf.nx, rm, rj, rp, cm, ck, cp, o, s_m, s_0, s_p);
         }
-        __syncthreads();
     }
+    __syncthreads();
+    if (owner) rr_accumulate(rtile + (ib & 1) * (R * TW), ib, a, I0, I1, Gf.nx, rm, rj, rp, cm, ck, cp, o, s_m, s_0, s_p);
+    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------------------------------

@@ -156,6 +156,11 @@ FUSED_LARGE = [
     ((33, 33, 129), 3, (1, 1, 1, 1, 0, 0), "fw", "jacobi"),
     ((65, 17, 97), 3, (0, 0, 1, 1, 1, 1), "fw", "gs"),
     ((33, 65, 65), 3, (0, 0, 1, 1, 1, 1), "inj", "gs"),
+    # long x: each block of the fused kernel marches several coarse planes, carrying the
+    # FullWeighting partial sums from one fine plane to the next
+    ((257, 33, 65), 3, (1, 1, 1, 1, 0, 0), "fw", "jacobi"),
+    ((513, 17, 33), 3, (0, 0, 1, 1, 1, 1), "fw", "gs"),
+    ((257, 17, 33), 3, (1, 1, 0, 0, 0, 0), "inj", "jacobi"),
 ]
 
 
@@ -172,6 +177,28 @@ def test_fused_setup_large_bit_exact(mgp_mod, gpu_ready, ci):
     for l in range(o.levels):
         assert_field_equal(o, e, "u", l)
         assert_field_equal(o, e, "f", l)
+
+
+@pytest.mark.parametrize("ci", [0, 3])
+def test_fused_setup_float_matches_unfused(mgp_mod, gpu_ready, ci):
+    """FP32: the one-kernel set-up gives the same bits as residual + restriction kernels."""
+    cfg = cfg_of(FUSED_LARGE[ci], h=1.0 / 128)
+    o = make_oracle(cfg)
+    randomize(o, 95 + ci)
+    engines = [make_engine(mgp_mod, cfg, dtype=mgp_mod.F32, flags=fl) for fl in (0, mgp_mod.FLAG_FUSED_SETUP)]
+    for e in engines:
+        for l in range(o.levels):
+            for name in ("u", "uprev", "f", "r"):
+                if name == "uprev" and o.relaxation != 0:
+                    continue
+                e.upload(name, o.field(name, l).astype(np.float32), l)
+            for fc in range(6):
+                e.upload_face(fc, o.face(fc, l).astype(np.float32), l)
+        e.fcycle(0, o.default_omega(), 2)
+    for l in range(o.levels):
+        for name in ("u", "f"):
+            a, b = engines[0].download(name, l), engines[1].download(name, l)
+            assert np.array_equal(a, b), (name, l)
 
 
 @pytest.mark.parametrize("ci", range(len(CONFIGS)))
