@@ -243,8 +243,14 @@ int mgp_batch_status(mgp_batch* b, int id, mgp_stats* out);
 /* Steps until every active problem has ||r||inf/||f||inf < tol (each problem stops when it
  * gets there) or maxiter steps; then stores every problem's FP64 residual. */
 int mgp_batch_solve(mgp_batch* b, double tol, int64_t maxiter, int64_t* steps);
-/* Kernel launches of one step for the current active set. */
+/* Kernel launches of one step for the current active set (for the latest non-empty active
+ * set once every problem has converged). */
 int mgp_batch_kernel_launches(const mgp_batch* b, int64_t* per_step);
+/* Device memory available to this batch: cudaMemGetInfo's free bytes plus what the batch's
+ * memory pool holds from retired problems (problems allocate from that pool, in the batch
+ * stream's order, and give their memory back to it on removal).  No counterpart in the
+ * reference, which has no batching. */
+int mgp_batch_mem_info(mgp_batch* b, size_t* free_bytes, size_t* total_bytes);
 
 /* Free and total device memory (cudaMemGetInfo) of `device`, for admission control. */
 int mgp_mem_info(int device, size_t* free_bytes, size_t* total_bytes);

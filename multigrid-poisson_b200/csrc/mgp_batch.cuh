@@ -185,6 +185,12 @@ struct mgp_batch {
     std::vector<BatchLaunch> launches;
     cudaGraphExec_t graph = nullptr;
     int64_t launches_total = 0;
+    int64_t launches_last = 0;  // launches of the latest non-empty schedule
+    // Problems allocate their hierarchies from this pool in the batch stream's order: memory
+    // of a retired problem goes back to the pool, not to the driver, so admitting and
+    // retiring never synchronise the device.  h_slab: 64 pinned bytes per slot.
+    cudaMemPool_t pool = nullptr;
+    unsigned long long* h_slab = nullptr;
 };
 
 namespace {
@@ -390,6 +396,7 @@ int batch_rebuild(mgp_batch* b) {
         CK(cudaMemcpyAsync(b->d_items, sb.bytes.data(), sb.bytes.size(), cudaMemcpyHostToDevice, b->stream));
     CK(cudaStreamSynchronize(b->stream));
     b->launches = sb.launches;
+    if (!b->launches.empty()) b->launches_last = (int64_t)b->launches.size();
     // capture the launch list once; replayed every step while the active set is unchanged
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -483,9 +490,24 @@ int mgp_batch_create(const mgp_batch_desc* d, mgp_batch** out) {
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_norms, sizeof(unsigned long long) * b->slots);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_norms, sizeof(unsigned long long) * b->slots);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_slab, 64 * (size_t)b->slots);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = b->device;
+        e = cudaMemPoolCreate(&b->pool, &props);
+        if (e != cudaSuccess) b->pool = nullptr;
+    }
+    if (e == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;  // memory freed into the pool stays reserved for the next problem
+        e = cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e != cudaSuccess) {
         if (b->d_norms) cudaFree(b->d_norms);
         if (b->h_norms) cudaFreeHost(b->h_norms);
+        if (b->h_slab) cudaFreeHost(b->h_slab);
+        if (b->pool) cudaMemPoolDestroy(b->pool);
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "batch set-up: %s", cudaGetErrorString(e));
@@ -501,9 +523,12 @@ int mgp_batch_destroy(mgp_batch* b) {
     batch_free_schedule(b);
     for (auto& p : b->probs)
         if (p.s) mgp_destroy(p.s);
+    cudaStreamSynchronize(b->stream);  // the problems' memory is back in the pool
+    if (b->pool) cudaMemPoolDestroy(b->pool);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_norms) cudaFree(b->d_norms);
     if (b->h_norms) cudaFreeHost(b->h_norms);
+    if (b->h_slab) cudaFreeHost(b->h_slab);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return MGP_OK;
@@ -543,14 +568,15 @@ int mgp_batch_add(mgp_batch* b, const mgp_desc* problem, int* id) {
     d.relaxation = b->desc.relaxation;
     d.prolongation = MGP_TRILINEAR;
     d.flags = (d.flags & MGP_FLAG_STRICT_BC) | (b->desc.inner_dtype == MGP_F32 ? MGP_FLAG_REFINE_F32 : MGP_FLAG_REFINE_F64);
-    mgp_solver* s = nullptr;
-    CKS(mgp_create(&d, &s));
     // slot: lowest free
     std::vector<char> taken(b->slots, 0);
     for (auto& p : b->probs)
         if (p.s) taken[p.slot] = 1;
     int slot = 0;
     while (slot < b->slots && taken[slot]) slot++;
+    mgp_solver* s = nullptr;
+    const CreateCtx ctx{b->stream, b->pool, b->h_slab + 8 * (size_t)slot};
+    CKS(create_solver(&d, &s, &ctx));
     BatchProblem p;
     p.id = b->next_id++;
     p.s = s;
@@ -684,7 +710,18 @@ int mgp_batch_solve(mgp_batch* b, double tol, int64_t maxiter, int64_t* steps) {
 
 int mgp_batch_kernel_launches(const mgp_batch* b, int64_t* per_step) {
     if (!b || !per_step) return fail(MGP_ERR_INVALID_ARG, "null argument");
-    *per_step = (int64_t)b->launches.size();
+    *per_step = b->launches.empty() ? b->launches_last : (int64_t)b->launches.size();
+    return MGP_OK;
+}
+
+int mgp_batch_mem_info(mgp_batch* b, size_t* free_bytes, size_t* total_bytes) {
+    if (!b || !free_bytes || !total_bytes) return fail(MGP_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(b->device);
+    CK(cudaMemGetInfo(free_bytes, total_bytes));
+    uint64_t reserved = 0, used = 0;
+    CK(cudaMemPoolGetAttribute(b->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    CK(cudaMemPoolGetAttribute(b->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    if (reserved > used) *free_bytes += (size_t)(reserved - used);
     return MGP_OK;
 }
 

@@ -123,9 +123,36 @@ struct mgp_solver {
     // inner solver shares this solver's stream.
     mgp_solver* inner = nullptr;
     bool owns_stream = true;
+    // Problems of a batch allocate from the batch's memory pool in the batch's stream order
+    // (no device-wide synchronisation when they come and go) and read norms back through the
+    // batch's pinned slab.
+    cudaMemPool_t pool = nullptr;
+    bool owns_h_norm = true;
+};
+
+// Where a solver's memory comes from: nullptr = its own stream, cudaMalloc, pinned read-back.
+struct CreateCtx {
+    cudaStream_t stream;
+    cudaMemPool_t pool;
+    unsigned long long* h_norm;  // 64 pinned bytes
 };
 
 namespace {
+
+// ---- device memory: cudaMalloc, or the batch pool in stream order ------------------------
+cudaError_t dev_alloc(mgp_solver* s, void** p, size_t bytes) {
+    if (s->pool) return cudaMallocFromPoolAsync(p, bytes, s->pool, s->stream);
+    return cudaMalloc(p, bytes);
+}
+void dev_free(mgp_solver* s, void* p) {
+    if (!p) return;
+    if (s->pool) cudaFreeAsync(p, s->stream);
+    else cudaFree(p);
+}
+cudaError_t dev_zero(mgp_solver* s, void* p, size_t bytes) {
+    if (s->pool) return cudaMemsetAsync(p, 0, bytes, s->stream);
+    return cudaMemset(p, 0, bytes);
+}
 
 // ---- state helpers ----------------------------------------------------------------------
 uint64_t state_bits(const mgp_solver* s) {
@@ -846,10 +873,10 @@ int copy_field_staged(mgp_solver* s, int l, void* dev, void* host, bool to_devic
     const size_t es = s->esize;
     const size_t bytes = (size_t)I.size * es;
     if (s->stage_bytes < bytes) {
-        if (s->stage) cudaFree(s->stage);
+        dev_free(s, s->stage);
         s->stage = nullptr;
         s->stage_bytes = 0;
-        CK(cudaMalloc(&s->stage, bytes));
+        CK(dev_alloc(s, &s->stage, bytes));
         s->stage_bytes = bytes;
     }
     if (to_device) {
@@ -930,14 +957,12 @@ void release(mgp_solver* s) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     s->graphs.clear();
     for (auto& L : s->lv) {
-        for (void* p : {L.ubuf[0], L.ubuf[1], L.f, L.r})
-            if (p) cudaFree(p);
-        for (void* p : L.face)
-            if (p) cudaFree(p);
+        for (void* p : {L.ubuf[0], L.ubuf[1], L.f, L.r}) dev_free(s, p);
+        for (void* p : L.face) dev_free(s, p);
     }
-    if (s->d_norm) cudaFree(s->d_norm);
-    if (s->h_norm) cudaFreeHost(s->h_norm);
-    if (s->stage) cudaFree(s->stage);
+    dev_free(s, s->d_norm);
+    if (s->h_norm && s->owns_h_norm) cudaFreeHost(s->h_norm);
+    dev_free(s, s->stage);
     if (s->inner) release(s->inner);
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1058,7 +1083,7 @@ int mgp_plan_level(const mgp_desc* d, int l, mgp_level_info* out) {
     return MGP_OK;
 }
 
-static int create_plain(const mgp_desc* d, mgp_solver** out) {
+static int create_plain(const mgp_desc* d, mgp_solver** out, const CreateCtx* ctx) {
     if (!d || !out) return fail(MGP_ERR_INVALID_ARG, "null descriptor or out pointer");
     *out = nullptr;
     std::vector<mgp_level_info> plan(d->levels > 0 && d->levels <= 30 ? d->levels : 1);
@@ -1079,6 +1104,17 @@ static int create_plain(const mgp_desc* d, mgp_solver** out) {
     const int64_t hw = plan[0].halo[1], hs = plan[0].halo[3], hb = plan[0].halo[5];
 
     DeviceGuard guard(s->device);
+    if (ctx) {
+        s->stream = ctx->stream;
+        s->owns_stream = false;
+        s->pool = ctx->pool;
+        s->h_norm = ctx->h_norm;
+        s->owns_h_norm = false;
+    } else if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        s->stream = nullptr;
+        release(s);
+        return fail(MGP_ERR_CUDA, "stream creation failed");
+    }
     s->lv.resize(s->levels);
     for (int l = 0; l < s->levels; l++) {
         LevelState& L = s->lv[l];
@@ -1107,22 +1143,21 @@ static int create_plain(const mgp_desc* d, mgp_solver** out) {
         const size_t bytes = L.elems * s->esize;
         const int nbuf = s->desc.relaxation == MGP_JACOBI ? 2 : 1;
         cudaError_t e = cudaSuccess;
-        for (int b = 0; b < nbuf && e == cudaSuccess; b++) e = cudaMalloc(&L.ubuf[b], bytes);
-        if (e == cudaSuccess) e = cudaMalloc(&L.f, bytes);
-        if (e == cudaSuccess) e = cudaMalloc(&L.r, bytes);
+        for (int b = 0; b < nbuf && e == cudaSuccess; b++) e = dev_alloc(s, &L.ubuf[b], bytes);
+        if (e == cudaSuccess) e = dev_alloc(s, &L.f, bytes);
+        if (e == cudaSuccess) e = dev_alloc(s, &L.r, bytes);
         for (int f = 0; f < 6 && e == cudaSuccess; f++)
-            e = cudaMalloc(&L.face[f], (size_t)(I.face_shape[f][0] * I.face_shape[f][1] * I.face_shape[f][2]) * s->esize);
+            e = dev_alloc(s, &L.face[f], (size_t)(I.face_shape[f][0] * I.face_shape[f][1] * I.face_shape[f][2]) * s->esize);
         if (e != cudaSuccess) {
             release(s);
             return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "allocating level %d: %s", l,
                         cudaGetErrorString(e));
         }
         for (void* p : {L.ubuf[0], L.ubuf[1], L.f, L.r})
-            if (p && e == cudaSuccess) e = cudaMemset(p, 0, bytes);
+            if (p && e == cudaSuccess) e = dev_zero(s, p, bytes);
         for (int f = 0; f < 6; f++)
             if (e == cudaSuccess)
-                e = cudaMemset(L.face[f], 0,
-                               (size_t)(I.face_shape[f][0] * I.face_shape[f][1] * I.face_shape[f][2]) * s->esize);
+                e = dev_zero(s, L.face[f], (size_t)(I.face_shape[f][0] * I.face_shape[f][1] * I.face_shape[f][2]) * s->esize);
         if (e != cudaSuccess) {
             release(s);
             return fail(MGP_ERR_CUDA, "zeroing level %d: %s", l, cudaGetErrorString(e));
@@ -1134,12 +1169,12 @@ static int create_plain(const mgp_desc* d, mgp_solver** out) {
         if (s->dtype == MGP_F64) tma_prepare_level<double>(s, s->lv[l]);
         else tma_prepare_level<float>(s, s->lv[l]);
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_norm, 64);
-    if (e == cudaSuccess) e = cudaMemset(s->d_norm, 0, 64);
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_norm, 64);
+    cudaError_t e = dev_alloc(s, (void**)&s->d_norm, 64);
+    if (e == cudaSuccess) e = dev_zero(s, s->d_norm, 64);
+    if (e == cudaSuccess && !s->h_norm) e = cudaMallocHost(&s->h_norm, 64);
     s->err_word = reinterpret_cast<int*>(reinterpret_cast<char*>(s->d_norm) + 8);
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    // a pooled solver's set-up is ordered on the shared stream; nothing to wait for here
+    if (e == cudaSuccess && !s->pool) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         release(s);
         return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "solver set-up: %s",
@@ -1149,11 +1184,11 @@ static int create_plain(const mgp_desc* d, mgp_solver** out) {
     return MGP_OK;
 }
 
-int mgp_create(const mgp_desc* d, mgp_solver** out) {
+static int create_solver(const mgp_desc* d, mgp_solver** out, const CreateCtx* ctx) {
     if (!d || !out) return fail(MGP_ERR_INVALID_ARG, "null descriptor or out pointer");
     *out = nullptr;
     const uint32_t refine = d->flags & (MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64);
-    if (!refine) return create_plain(d, out);
+    if (!refine) return create_plain(d, out, ctx);
     if (refine == (MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64))
         return fail(MGP_ERR_INVALID_ARG, "choose one of MGP_FLAG_REFINE_F32 / MGP_FLAG_REFINE_F64");
     if (d->dtype != MGP_F64) return fail(MGP_ERR_INVALID_ARG, "a refinement solver keeps level 0 in FP64 (dtype F64)");
@@ -1167,22 +1202,23 @@ int mgp_create(const mgp_desc* d, mgp_solver** out) {
     dout.flags &= ~(MGP_FLAG_REFINE_F32 | MGP_FLAG_REFINE_F64);
     dout.levels = 1;
     mgp_solver* outer = nullptr;
-    CKS(create_plain(&dout, &outer));
+    CKS(create_plain(&dout, &outer, ctx));
+    // the inner hierarchy shares the outer solver's stream (and memory pool)
     mgp_solver* inner = nullptr;
-    int st = create_plain(&di, &inner);
+    CreateCtx ictx{outer->stream, outer->pool, outer->h_norm};
+    int st = create_plain(&di, &inner, &ictx);
     if (st != MGP_OK) {
         release(outer);
         return st;
     }
-    cudaStreamDestroy(inner->stream);
-    inner->stream = outer->stream;
-    inner->owns_stream = false;
     inner->err_word = outer->err_word;  // seen by the outer solver's norm read-back
     outer->inner = inner;
     outer->desc = *d;  // keeps the refine flag and the user's level count
     *out = outer;
     return MGP_OK;
 }
+
+int mgp_create(const mgp_desc* d, mgp_solver** out) { return create_solver(d, out, nullptr); }
 
 int mgp_destroy(mgp_solver* s) {
     if (!s) return MGP_OK;

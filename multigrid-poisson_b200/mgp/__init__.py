@@ -130,6 +130,7 @@ def lib():
         L.mgp_batch_status.argtypes = [vp, i32, ctypes.POINTER(Stats)]
         L.mgp_batch_solve.argtypes = [vp, dbl, i64, ctypes.POINTER(i64)]
         L.mgp_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(i64)]
+        L.mgp_batch_mem_info.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
         L.mgp_mem_info.argtypes = [i32, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
         dp = ctypes.POINTER(dbl)
         L.mgp_fill_sine_modes.argtypes = [vp, i32, dp, dp, dp, dp, dp]
@@ -463,6 +464,13 @@ class Batch:
         k = ctypes.c_int64()
         _check(lib().mgp_batch_kernel_launches(self._h, ctypes.byref(k)))
         return k.value
+
+    def mem_info(self):
+        """(free, total) device bytes available to this batch: the device's free memory plus
+        what the batch's memory pool keeps from retired problems."""
+        f, t = ctypes.c_size_t(), ctypes.c_size_t()
+        _check(lib().mgp_batch_mem_info(self._h, ctypes.byref(f), ctypes.byref(t)))
+        return f.value, t.value
 
 
 # ----------------------------------------------------------------------------------------

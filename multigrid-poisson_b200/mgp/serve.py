@@ -4,14 +4,16 @@ Requests (grid dims, boundary kinds, a right-hand side given by sine modes, tole
 arrive over time.  The server loop:
 
 * admits arrived requests while the device has memory for them (free HBM from
-  cudaMemGetInfo minus a reserve, per-problem bytes from mgp_batch_problem_bytes) and the
-  batch has a free slot; an admitted request's hierarchy stays resident until it finishes,
-  and its right-hand side is generated on the device;
+  cudaMemGetInfo plus what the batch's memory pool holds from retired requests, minus a
+  reserve; per-problem bytes from mgp_batch_problem_bytes) and the batch has a free slot; an
+  admitted request's hierarchy stays resident until it finishes, and its right-hand side is
+  generated on the device;
 * runs one batched refinement step (mgp_batch_step) for every resident request -- each
   level operation of every request is one persistent kernel over a (request, tile) work
   list, so requests of different sizes share launches;
 * retires requests whose FP64 relative residual ||r||inf/||f||inf is below their
-  tolerance: the solution comes back to the host and the slot and memory free up.
+  tolerance: the solution comes back to the host (into a reused page-locked buffer) and the
+  slot and memory free up.
 
 Requests that arrive while others are on the GPU join at the next step boundary (continuous
 batching, not a queue in front of a one-at-a-time solver).  Latency = finish - arrival.
@@ -25,7 +27,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import F32, F64, FULLWEIGHTING, GAUSSSEIDEL, Batch, mem_info
+from . import F32, F64, FULLWEIGHTING, GAUSSSEIDEL, Batch, host_array
 
 KINDS = ("dirichlet", "neumann", "mixed")
 
@@ -100,7 +102,7 @@ def make_stream(n: int, rate: float, seed: int = 0, **kw) -> list:
 
 class Server:
     def __init__(self, inner=F32, max_batch=64, reserve_bytes=4 << 30, device=0, max_steps=200,
-                 keep_solutions=False, nsmooth=2):
+                 keep_solutions=False, nsmooth=2, digest=False):
         self.batch = Batch(FULLWEIGHTING, GAUSSSEIDEL, inner, "Fcycle", nsmooth, max_problems=max_batch,
                            device=device)
         self.max_batch = max_batch
@@ -108,15 +110,17 @@ class Server:
         self.device = device
         self.max_steps = max_steps
         self.keep = keep_solutions
+        self.digest = digest
         self.steps = 0
         self.batch_sizes = []
+        self._landing = None  # page-locked download buffer, grown to the largest solution
 
     def close(self):
         self.batch.close()
 
     def _admit(self, req: Request, now: float) -> bool:
         need = self.batch.problem_bytes(req.dims, req.levels, req.h, req.bc)
-        free, _ = mem_info(self.device)
+        free, _ = self.batch.mem_info()
         if free - need < self.reserve:
             return False
         pid = self.batch.add(req.dims, req.levels, req.h, req.bc)
@@ -129,10 +133,25 @@ class Server:
     def _retire(self, pid: int, req: Request, now: float):
         st = self.batch.status(pid)
         req.iterations, req.rel_res = int(st.iterations), st.rel_res
-        u = self.batch.problem(pid).download("u", 0)
-        req.digest = hashlib.sha256(u.tobytes()).hexdigest()[:16]
+        s = self.batch.problem(pid)
+        lv = s.level[0]
+        if self._landing is None or self._landing.size < lv.size:
+            self._landing = host_array((lv.size,), s.np_dtype, pinned=True)
+        u = self._landing[:lv.size].reshape(lv.pad)
+        # the download writes the shape points; the halo of the reused buffer is zeroed so
+        # the result is what a fresh zeroed array would hold
+        ix, iy, iz = lv.interior
+        u[:ix.start] = 0
+        u[ix.stop:] = 0
+        u[:, :iy.start] = 0
+        u[:, iy.stop:] = 0
+        u[:, :, :iz.start] = 0
+        u[:, :, iz.stop:] = 0
+        s.download("u", 0, out=u)
+        if self.digest:
+            req.digest = hashlib.sha256(u.tobytes()).hexdigest()[:16]
         if self.keep:
-            req.solution = u
+            req.solution = u.copy()
         self.batch.remove(pid)
         req.finished = now
 
