@@ -50,7 +50,7 @@ struct TStencil {
 template <typename T>
 struct TRestrict {
     using Args = RestrictArgs<T>;
-    static __device__ __forceinline__ void run(const Args& a, int bx, int, int gx) { restrict_tile(a, bx, gx); }
+    static __device__ __forceinline__ void run(const Args& a, int bx, int by, int) { restrict_tile(a, bx, by); }
 };
 template <typename T>
 struct TBc {
@@ -65,7 +65,7 @@ struct TProlongAdd {
 template <typename Ti>
 struct TUpdate {
     using Args = UpdateArgs<double, Ti>;
-    static __device__ __forceinline__ void run(const Args& a, int bx, int, int gx) { refine_update_tile(a, bx, gx); }
+    static __device__ __forceinline__ void run(const Args& a, int bx, int by, int) { refine_update_tile(a, bx, by); }
 };
 template <typename Ti>
 struct TRefRes {
@@ -264,7 +264,8 @@ int build_step(mgp_batch* b, ScheduleBuilder& sb) {
             push_item(res, a, gx, gy);
             long long n = 0;
             auto ra = restrict_args<Ti>(in, l, true, &n);
-            push_item(rst, ra, (int)((n + kThreads - 1) / kThreads), 1);
+            const Geom& Gc = in->lv[l + 1].G;
+            push_item(rst, ra, (Gc.ny * Gc.nz + kThreads - 1) / kThreads, Gc.nx);
             bool any = false;
             auto ba = bc_args<Ti>(in, l, &any);
             if (any) {
@@ -337,9 +338,9 @@ int build_step(mgp_batch* b, ScheduleBuilder& sb) {
         mgp_solver* in = s->inner;
         LevelState& L = s->lv[0];
         LevelState& I = in->lv[0];
-        const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
         UpdateArgs<double, Ti> ua{(double*)u_ptr(s, 0), L.G, (const Ti*)u_ptr(in, 0), I.G.sx, I.G.sy};
-        push_item(ups, ua, (int)((n + kThreads - 1) / kThreads), 1);
+        constexpr int Vd = VecT<double>::V;
+        push_item(ups, ua, (L.G.ny * ((L.G.nz + Vd - 1) / Vd) + kThreads - 1) / kThreads, L.G.nx);
         RefineArgs<double, Ti> ra;
         ra.G = L.G;
         ra.u = (const double*)u_ptr(s, 0);

@@ -484,7 +484,8 @@ template <typename T>
 int restrict_t(mgp_solver* s, int l, bool zero_coarse_u) {
     long long n = 0;
     RestrictArgs<T> a = restrict_args<T>(s, l, zero_coarse_u, &n);
-    return launch_k(s, k_restrict<T>, dim3(grid_1d(s, n)), dim3(kThreads), 0, a);
+    const LevelState& C = s->lv[l + 1];
+    return launch_k(s, k_restrict<T>, dim3((C.G.ny * C.G.nz + kThreads - 1) / kThreads, C.G.nx), dim3(kThreads), 0, a);
 }
 
 template <typename T>
@@ -532,8 +533,9 @@ int zero_u_t(mgp_solver* s, int l) {
 template <typename T>
 int norm_t(mgp_solver* s, const void* a, int l, unsigned long long* out) {
     LevelState& L = s->lv[l];
-    const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
-    return launch_k(s, k_norm<T>, dim3(grid_1d(s, n)), dim3(kThreads), 0, (const T*)a, L.G, out);
+    const int bx = (L.G.ny * L.G.nz + kThreads - 1) / kThreads;
+    const int chunks = std::max(1, std::min(L.G.nx, sm_count(s->device) * 8 / bx));
+    return launch_k(s, k_norm<T>, dim3(bx, chunks), dim3(kThreads), 0, (const T*)a, L.G, out);
 }
 
 template <typename T>
@@ -784,9 +786,10 @@ int refine_update_t(mgp_solver* s) {
     mgp_solver* in = s->inner;
     LevelState& L = s->lv[0];
     LevelState& I = in->lv[0];
-    const long long n = (long long)L.G.nx * L.G.ny * L.G.nz;
+    constexpr int V = VecT<double>::V;
     UpdateArgs<double, Ti> a{(double*)u_ptr(s, 0), L.G, (const Ti*)u_ptr(in, 0), I.G.sx, I.G.sy};
-    return launch_k(s, k_refine_update<double, Ti>, dim3(grid_1d(s, n)), dim3(kThreads), 0, a);
+    const int bx = (L.G.ny * ((L.G.nz + V - 1) / V) + kThreads - 1) / kThreads;
+    return launch_k(s, k_refine_update<double, Ti>, dim3(bx, L.G.nx), dim3(kThreads), 0, a);
 }
 
 int refine_residual(mgp_solver* s, bool write_r) {

@@ -179,6 +179,26 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// cp.async of one 4- or 8-byte element (the L1-allocating form is the only one below 16 bytes)
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"((int)sizeof(T)) : "memory");
+}
+
+// Stage the V-vector at offset o: f, except at the elements in `unr`, which take r.
+template <typename T, int V>
+__device__ __forceinline__ void stage_f_or_r(T* slot, const T* f, const T* r, long long o, unsigned unr) {
+    if (!unr) {
+        cp_async16(slot, f + o);
+    } else if (unr == (1u << V) - 1u) {
+        cp_async16(slot, r + o);
+    } else {
+#pragma unroll
+        for (int e = 0; e < V; e++) cp_async_elem(slot + e, ((unr >> e) & 1u) ? r + o + e : f + o + e);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void lds_v(T (&d)[VecT<T>::V], const T* p) {
 #pragma unroll
@@ -197,6 +217,7 @@ template <typename T, int OP, bool NORM>
 __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int bx, const int by) {
     constexpr int V = VecT<T>::V;
     __shared__ __align__(16) T stage_u[kStages][256 * V];
+    // f; with NORM, the stored r in place of f at the vector's unrelaxed points
     __shared__ __align__(16) T stage_f[kStages][256 * V];
     const Geom& G = a.G;
     const int nv = (G.nz + V - 1) / V;
@@ -241,6 +262,8 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
             const T m2h = -two_h;
             T* su = &stage_u[0][threadIdx.x * V];
             T* sf = &stage_f[0][threadIdx.x * V];
+            const unsigned unr = NORM ? (ins & ~inr) : 0u;  // r staged at these elements
+            const T* rr = a.dst;
             constexpr int SS = 256 * V;  // stage stride
             // stage s holds u(i0+s+1) and f(i0+s)
 #pragma unroll
@@ -248,7 +271,7 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                 const int p = i0 + st;
                 if (p < i1) {
                     if (p + 1 < G.nx) cp_async16(su + st * SS, src + (long long)(p + 1) * G.sx + bjk);
-                    cp_async16(sf + st * SS, f + (long long)p * G.sx + bjk);
+                    stage_f_or_r<T, V>(sf + st * SS, f, rr, (long long)p * G.sx + bjk, unr);
                 }
                 cp_async_commit();
             }
@@ -278,11 +301,16 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                                                   : T(0);
                 }
                 lds_v(fc, sf + slot * SS);
+                if (NORM && unr) {  // stored r at the unrelaxed points of this plane
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if ((unr >> e) & 1u) mx = max(mx, abs_bits(fc[e]));
+                }
                 {  // refill this slot with plane i+kStages
                     const int q = i + kStages;
                     if (q < i1) {
                         if (q + 1 < G.nx) cp_async16(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
-                        cp_async16(sf + slot * SS, f + (long long)q * G.sx + bjk);
+                        stage_f_or_r<T, V>(sf + slot * SS, f, rr, (long long)q * G.sx + bjk, unr);
                     }
                     cp_async_commit();
                 }
@@ -292,12 +320,6 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
 #pragma unroll
                     for (int e = 0; e < V; e++)
                         if (((base + e) & 1) != a.colour) act &= ~(1u << e);
-                }
-                if (NORM && (ins & ~inr)) {  // stored r at the unrelaxed points of this plane
-                    const T* rp = a.dst + p;
-#pragma unroll
-                    for (int e = 0; e < V; e++)
-                        if (((ins & ~inr) >> e) & 1u) mx = max(mx, abs_bits(rp[e]));
                 }
                 T cur[V];
 #pragma unroll
@@ -424,29 +446,27 @@ struct RestrictArgs {
     int fw;
 };
 
-// coarse points bx*256 + tid, bx*256 + tid + gx*256, ...
+// Coarse plane `i` (the tile's y index), coarse points j*n[2]+k = bx*256 + thread of it.
 template <typename T>
-__device__ __forceinline__ void restrict_tile(const RestrictArgs<T>& a, const int bx, const int gx) {
+__device__ __forceinline__ void restrict_tile(const RestrictArgs<T>& a, const int bx, const int i) {
     const View vo = a.vo;
-    const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
-    for (long long t = bx * 256ll + threadIdx.x; t < n; t += gx * 256ll) {
-        const int k = (int)(t % vo.n[2]);
-        const long long q = t / vo.n[2];
-        const int j = (int)(q % vo.n[1]);
-        const int i = (int)(q / vo.n[1]);
-        const long long o = i * vo.s0 + j * vo.s1 + k;
-        T v;
-        if (a.fw) v = fw_point(a.in, a.vi, i, j, k);
-        else v = ldg(a.in + (2 * i) * a.vi.s0 + (2 * j) * a.vi.s1 + 2 * k);  // injection.h:63
-        a.out[o] = v;
-        if (a.zero_u) a.zero_u[o] = T(0);
-    }
+    const int t = bx * 256 + (int)threadIdx.x;
+    if (t >= vo.n[1] * vo.n[2]) return;
+    const int j = t / vo.n[2];
+    const int k = t - j * vo.n[2];
+    const long long o = i * vo.s0 + j * vo.s1 + k;
+    T v;
+    if (a.fw) v = fw_point(a.in, a.vi, i, j, k);
+    else v = ldg(a.in + (2 * i) * a.vi.s0 + (2 * j) * a.vi.s1 + 2 * k);  // injection.h:63
+    a.out[o] = v;
+    if (a.zero_u) a.zero_u[o] = T(0);
 }
 
+// grid: ((n[1]*n[2] + 255)/256, n[0]) of the coarse view
 template <typename T>
 __global__ void __launch_bounds__(256) k_restrict(RestrictArgs<T> a) {
     pdl_begin();
-    restrict_tile(a, blockIdx.x, gridDim.x);
+    restrict_tile(a, blockIdx.x, blockIdx.y);
 }
 
 // Neumann::restrict_to (include/neumann.h:146-252) for every Neumann face of the coarse
@@ -626,12 +646,6 @@ constexpr size_t rr_smem_bytes(int tkv, int rows) {
            sizeof(T);
 }
 
-// cp.async of one 4- or 8-byte element (the L1-allocating form is the only one below 16 bytes)
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"((int)sizeof(T)) : "memory");
-}
 // 16-byte cp.async that bypasses L1 (the block reads the data from shared memory only)
 __device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -1016,18 +1030,18 @@ __global__ void __launch_bounds__(256) k_add(T* u, const T* __restrict__ r, Geom
     }
 }
 
-// max |a| over the shape (DeviceArray::infinity_norm).
+// max |a| over the shape (DeviceArray::infinity_norm).  grid: ((ny*nz + 255)/256, chunks of
+// planes); each thread reads one (j, k) column of its block's planes.
 template <typename T>
 __global__ void __launch_bounds__(256) k_norm(const T* __restrict__ a, Geom G, unsigned long long* out) {
     pdl_begin();
-    const long long n = (long long)G.nx * G.ny * G.nz;
+    const int t = blockIdx.x * 256 + (int)threadIdx.x;
     unsigned long long mx = 0ull;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t % G.nz);
-        const long long q = t / G.nz;
-        const int j = (int)(q % G.ny);
-        const int i = (int)(q / G.ny);
-        mx = max(mx, abs_bits(ldg(a + (long long)i * G.sx + (long long)j * G.sy + k)));
+    if (t < G.ny * G.nz) {
+        const int j = t / G.nz;
+        const int k = t - j * G.nz;
+        const T* col = a + (long long)j * G.sy + k;
+        for (int i = blockIdx.y; i < G.nx; i += gridDim.y) mx = max(mx, abs_bits(ldg(col + (long long)i * G.sx)));
     }
     block_max_to(mx, out);
 }
@@ -1179,28 +1193,53 @@ struct UpdateArgs {
     long long sxi, syi;
 };
 
+// V values of e (type Ti) at an offset that is a multiple of V (rows of the inner level are
+// 64-byte aligned): one 16-byte load, or one 8-byte load for V floats next to V doubles.
+__device__ __forceinline__ void ld_corr(double (&d)[2], const double* p) { ldv(d, p); }
+__device__ __forceinline__ void ld_corr(double (&d)[2], const float* p) {
+    const float2 x = __ldg(reinterpret_cast<const float2*>(p));
+    d[0] = (double)x.x;
+    d[1] = (double)x.y;
+}
+__device__ __forceinline__ void ld_corr(float (&d)[4], const float* p) { ldv(d, p); }
+
+// Plane i (the tile's y index): one thread per k-vector of a row, u += (T) e where
+// (i, j, k) is inside the relaxation bounds.
 template <typename T, typename Ti>
-__device__ __forceinline__ void refine_update_tile(const UpdateArgs<T, Ti>& a, const int bx, const int gx) {
-    T* u = a.u;
+__device__ __forceinline__ void refine_update_tile(const UpdateArgs<T, Ti>& a, const int bx, const int i) {
+    constexpr int V = VecT<T>::V;
     const Geom& G = a.G;
-    const Ti* __restrict__ e = a.e;
-    const long long sxi = a.sxi, syi = a.syi;
-    const long long n = (long long)G.nx * G.ny * G.nz;
-    for (long long t = bx * 256ll + threadIdx.x; t < n; t += gx * 256ll) {
-        const int k = (int)(t % G.nz);
-        const long long q = t / G.nz;
-        const int j = (int)(q % G.ny);
-        const int i = (int)(q / G.ny);
-        if (i < G.x0 || i >= G.x1 || j < G.y0 || j >= G.y1 || k < G.z0 || k >= G.z1) continue;
-        const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
-        u[p] = u[p] + (T)ldg(e + (long long)i * sxi + (long long)j * syi + k);
+    const int nv = (G.nz + V - 1) / V;
+    const int t = bx * 256 + (int)threadIdx.x;
+    if (t >= G.ny * nv || i < G.x0 || i >= G.x1) return;
+    const int j = t / nv;
+    const int kb = (t - j * nv) * V;
+    if (j < G.y0 || j >= G.y1) return;
+    unsigned act = 0u;
+#pragma unroll
+    for (int e = 0; e < V; e++)
+        if (kb + e >= G.z0 && kb + e < G.z1) act |= 1u << e;
+    if (!act) return;
+    T* up = a.u + (long long)i * G.sx + (long long)j * G.sy + kb;
+    T c[V], u[V];
+    ld_corr(c, a.e + (long long)i * a.sxi + (long long)j * a.syi + kb);
+    ldv_rw(u, up);
+#pragma unroll
+    for (int e = 0; e < V; e++) u[e] = u[e] + c[e];
+    if (act == (1u << V) - 1u) {
+        stv(up, u);
+    } else {
+#pragma unroll
+        for (int e = 0; e < V; e++)
+            if ((act >> e) & 1u) up[e] = u[e];
     }
 }
 
+// grid: ((ny * ceil(nz/V) + 255)/256, nx)
 template <typename T, typename Ti>
 __global__ void __launch_bounds__(256) k_refine_update(UpdateArgs<T, Ti> a) {
     pdl_begin();
-    refine_update_tile(a, blockIdx.x, gridDim.x);
+    refine_update_tile(a, blockIdx.x, blockIdx.y);
 }
 
 // Device-side right-hand side: a sum of separable sine modes at the grid points.

@@ -160,6 +160,8 @@ class Server:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
         self._active = {}
+        self.steps = 0
+        self.batch_sizes = []
         t0 = clock()
         while pending or waiting or self._active:
             now = clock() - t0
