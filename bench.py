@@ -371,7 +371,7 @@ def bench_batched(mgp, torch, device=0, count=256, tol=1e-8):
     return out
 
 
-def bench_served(mgp, device=0, count=48, rates=(50.0, 2000.0), seed=0):
+def bench_served(mgp, device=0, count=120, rates=(50.0, 2000.0), seed=0):
     """Open-loop Poisson arrivals of `count` requests at each rate: boxes 2^k+1 per axis
     (k in 5..9 for x and y, 5..8 for z), Dirichlet / Neumann / mixed, 8 random sine modes,
     tolerance 1e-8; continuous batching with admission by free HBM.  A bounded sample of the
@@ -500,7 +500,7 @@ def main():
     ap.add_argument("--kernels", action="store_true", help="time each level-0 kernel alone")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the mixed-precision, batched and served workloads")
-    ap.add_argument("--served-requests", type=int, default=48)
+    ap.add_argument("--served-requests", type=int, default=120)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
