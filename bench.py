@@ -476,7 +476,22 @@ def run_reference_arm(args):
     # at most REF_ARM_CYCLES timed cycles (after at most 2 warm-up cycles) keep the run to a
     # minute or so whatever --steps says; the metric is per cycle, so the sample size does not
     # change it.
-    res = cpu_reference(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2))
+    nproc = os.cpu_count() or 1
+    # Thread sweep 1, 2, 4, ..., nproc: one timed cycle each below nproc (the reference's
+    # OpenMP build can be slower with more threads), the full sample at nproc; the line's
+    # value is the fastest.
+    sweep = {}
+    t = 1
+    while t < nproc:
+        r = cpu_reference(1, 0, threads=t)
+        sweep[t] = r["value"]
+        t *= 2
+    res = cpu_reference(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2), threads=nproc)
+    sweep[nproc] = res["value"]
+    best_t = max(sweep, key=sweep.get)
+    if best_t != nproc:
+        res = cpu_reference(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2), threads=best_t)
+        sweep[best_t] = max(sweep[best_t], res["value"])
     cores = res["threads"]
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(1, res["cycles"]),
@@ -485,7 +500,8 @@ def run_reference_arm(args):
             "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": f"{int(res['cycles'])} F-cycles on the full grid after {args.warmup} "
                                        f"warm-up cycles, OMP_NUM_THREADS={cores}"},
-            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "thread_sweep": {str(k): v for k, v in sorted(sweep.items())}}
     print(json.dumps(line))
     return 0
 

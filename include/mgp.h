@@ -160,6 +160,20 @@ int mgp_download_field(mgp_solver* s, int field, int level, void* host, int64_t 
 /* Boundary<T>::arr to_device (dirichlet.h:232-235, neumann.h:511-514) and back. */
 int mgp_upload_face(mgp_solver* s, int face, int level, const void* host, int64_t count);
 int mgp_download_face(mgp_solver* s, int face, int level, void* host, int64_t count);
+/* External coupling on the device (the role DeviceArray::devptr plays for codes such as
+ * include/poisson_helpers.h:8-34, which fill get_rhs / get_*_bc between init_zero and
+ * to_device): the device buffer that holds `field` of `level`, so a caller's own kernels can
+ * write or read it without a host round trip.  The layout is the engine's, not the
+ * reference's padded host layout: shape points only, k unit-stride,
+ *   element (i,j,k) at ptr[i*layout[3] + j*layout[4] + k],  layout = {nx, ny, nz, sx, sy}.
+ * The pointer stays valid until the solver is destroyed, but for MGP_FIELD_U / UPREV of a
+ * Jacobi solver it names the buffer that holds the field NOW: every sweep swaps the pair, so
+ * ask again after relaxing or solving.  Work on the returned memory must be ordered with the
+ * solver's stream (mgp_get_stream) by the caller. */
+int mgp_field_device(mgp_solver* s, int field, int level, void** ptr, int64_t layout[5]);
+/* The same for a face array of `level` (dense, the reference's face layout of shape
+ * shape[0] x shape[1] x shape[2], k unit-stride). */
+int mgp_face_device(mgp_solver* s, int face, int level, void** ptr, int64_t shape[3]);
 /* Domain<T>::write_bc_to(u) and (u_prev) as done at the end of Domain::to_device
  * (include/domain.h:259-262, 318-326): Dirichlet face data into the boundary planes, in
  * the reference's face order so that later faces win on shared edges. */

@@ -1278,6 +1278,30 @@ static int face_io(mgp_solver* s, int face, int l, void* host, int64_t count, bo
 int mgp_upload_face(mgp_solver* s, int face, int l, const void* host, int64_t count) {
     return face_io(s, face, l, const_cast<void*>(host), count, true);
 }
+int mgp_field_device(mgp_solver* s, int field, int l, void** ptr, int64_t layout[5]) {
+    CKS(validate_level(s, l));
+    if (!ptr || !layout) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
+    void* dev = field_ptr(s, field, l);
+    if (!dev) return fail(MGP_ERR_INVALID_ARG, "bad field %d", field);
+    const Geom& G = s->lv[l].G;
+    *ptr = dev;
+    layout[0] = G.nx;
+    layout[1] = G.ny;
+    layout[2] = G.nz;
+    layout[3] = G.sx;
+    layout[4] = G.sy;
+    return MGP_OK;
+}
+
+int mgp_face_device(mgp_solver* s, int face, int l, void** ptr, int64_t shape[3]) {
+    CKS(validate_level(s, l));
+    if (!ptr || !shape) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
+    if (face < 0 || face > 5) return fail(MGP_ERR_INVALID_ARG, "bad face %d", face);
+    *ptr = s->lv[l].face[face];
+    for (int k = 0; k < 3; k++) shape[k] = s->lv[l].face_shape[face][k];
+    return MGP_OK;
+}
+
 int mgp_download_face(mgp_solver* s, int face, int l, void* host, int64_t count) {
     return face_io(s, face, l, host, count, false);
 }

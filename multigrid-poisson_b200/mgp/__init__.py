@@ -107,6 +107,8 @@ def lib():
         L.mgp_num_levels.argtypes = [vp]
         for n in ("mgp_upload_field", "mgp_download_field", "mgp_upload_face", "mgp_download_face"):
             getattr(L, n).argtypes = [vp, i32, i32, vp, i64]
+        L.mgp_field_device.argtypes = [vp, i32, i32, ctypes.POINTER(vp), ctypes.POINTER(i64)]
+        L.mgp_face_device.argtypes = [vp, i32, i32, ctypes.POINTER(vp), ctypes.POINTER(i64)]
         L.mgp_write_bc.argtypes = [vp, i32]
         L.mgp_solve.argtypes = [vp, i32, i64, dbl, ctypes.c_char_p, dbl, ctypes.c_uint32, ctypes.POINTER(Stats)]
         L.mgp_set_iteration_limits.argtypes = [vp, i64, i64, dbl]
@@ -205,6 +207,19 @@ class Level:
         return (slice(hw, hw + nx), slice(hs, hs + ny), slice(hb, hb + nz))
 
 
+class DeviceView:
+    """A solver's device buffer described by __cuda_array_interface__ (version 3); keeps the
+    solver alive while the view exists."""
+
+    def __init__(self, ptr, shape, strides, dtype, owner):
+        self.ptr, self.shape, self.strides, self.dtype, self._owner = ptr, shape, strides, np.dtype(dtype), owner
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": self.shape, "strides": self.strides, "typestr": self.dtype.str, "data": (self.ptr, False),
+                "version": 3, "stream": None}
+
+
 class Solver:
     """One level hierarchy on one GPU, driven through the C ABI."""
 
@@ -284,6 +299,26 @@ class Solver:
         a = np.zeros(self.level[level].face_shape[fcid], dtype=self.np_dtype)
         _check(lib().mgp_download_face(self._h, fcid, level, a.ctypes.data, a.size))
         return a
+
+    def device_field(self, name, level=0) -> "DeviceView":
+        """The device buffer holding field `name` of `level`, as an object with
+        __cuda_array_interface__ (torch.as_tensor / cupy.asarray wrap it without a copy):
+        shape (nx, ny, nz), k unit-stride, the engine's row and plane pitches.  For u / uprev of
+        a Jacobi solver it is the buffer that holds the field now; every sweep swaps the pair."""
+        p = ctypes.c_void_p()
+        lay = (ctypes.c_int64 * 5)()
+        _check(lib().mgp_field_device(self._h, self._fid(name), level, ctypes.byref(p), lay))
+        es = np.dtype(self.np_dtype).itemsize
+        return DeviceView(p.value, (lay[0], lay[1], lay[2]), (lay[3] * es, lay[4] * es, es), self.np_dtype, self)
+
+    def device_face(self, fc, level=0) -> "DeviceView":
+        """The device face array `fc` of `level` (dense, the reference's face layout)."""
+        p = ctypes.c_void_p()
+        shp = (ctypes.c_int64 * 3)()
+        _check(lib().mgp_face_device(self._h, self._face_id(fc), level, ctypes.byref(p), shp))
+        es = np.dtype(self.np_dtype).itemsize
+        shape = (shp[0], shp[1], shp[2])
+        return DeviceView(p.value, shape, (shape[1] * shape[2] * es, shape[2] * es, es), self.np_dtype, self)
 
     def write_bc(self, level=0):
         _check(lib().mgp_write_bc(self._h, level))
