@@ -186,6 +186,7 @@ struct mgp_batch {
     cudaGraphExec_t graph = nullptr;
     int64_t launches_total = 0;
     int64_t launches_last = 0;  // launches of the latest non-empty schedule
+    int stable_steps = 0;       // steps run since the active set last changed
     // Problems allocate their hierarchies from this pool in the batch stream's order: memory
     // of a retired problem goes back to the pool, not to the driver, so admitting and
     // retiring never synchronise the device.  h_slab: 64 pinned bytes per slot.
@@ -398,7 +399,23 @@ int batch_rebuild(mgp_batch* b) {
     CK(cudaStreamSynchronize(b->stream));
     b->launches = sb.launches;
     if (!b->launches.empty()) b->launches_last = (int64_t)b->launches.size();
-    // capture the launch list once; replayed every step while the active set is unchanged
+    b->dirty = false;
+    return MGP_OK;
+}
+
+// One step's launches issued directly on the batch stream: the steps right after the active
+// set changed run this way (capturing and instantiating a graph of a few hundred launches
+// costs more than launching them a few times; the host issues them while the GPU works).
+constexpr int kBatchCaptureAfter = 3;
+int batch_launch_direct(mgp_batch* b) {
+    CK(cudaMemsetAsync(b->d_norms, 0, sizeof(unsigned long long) * b->slots, b->stream));
+    for (auto& L : b->launches) L.fn((const char*)b->d_items + L.offset, L.n, L.total, L.grid, b->stream);
+    CK(cudaGetLastError());
+    return MGP_OK;
+}
+
+// Capture of the current schedule, replayed every step while the active set stays the same.
+int batch_capture(mgp_batch* b) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     // the step's last launch max-reduces each problem's residual into its slot
@@ -418,8 +435,10 @@ int batch_rebuild(mgp_batch* b) {
     }
     cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
-    if (ei != cudaSuccess) return fail(MGP_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ei));
-    b->dirty = false;
+    if (ei != cudaSuccess) {
+        b->graph = nullptr;
+        return fail(MGP_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ei));
+    }
     return MGP_OK;
 }
 
@@ -634,12 +653,20 @@ int mgp_batch_step(mgp_batch* b, int* n_active) {
     CKS(batch_start_new(b));
     std::vector<uint64_t> cur;
     for (auto& p : b->probs) cur.push_back(p.s ? state_bits(p.s->inner) : 0);
-    if (b->dirty || cur != b->sched_state) CKS(batch_rebuild(b));
+    const bool changed = b->dirty || cur != b->sched_state;
+    if (changed) {
+        CKS(batch_rebuild(b));  // schedule only
+        b->stable_steps = 0;
+    } else if (!b->graph && !b->launches.empty() && b->stable_steps >= kBatchCaptureAfter) {
+        CKS(batch_capture(b));  // the set has held for a while: replay it as a graph
+    }
+    b->stable_steps++;
     int n = 0;
     for (auto& p : b->probs) n += (p.s && p.active && p.started);
     if (n_active) *n_active = n;
-    if (!n || !b->graph) return MGP_OK;
-    CK(cudaGraphLaunch(b->graph, b->stream));
+    if (!n || b->launches.empty()) return MGP_OK;
+    if (b->graph) CK(cudaGraphLaunch(b->graph, b->stream));
+    else CKS(batch_launch_direct(b));
     b->launches_total += (int64_t)b->launches.size();
     CK(cudaMemcpyAsync(b->h_norms, b->d_norms, sizeof(unsigned long long) * b->slots, cudaMemcpyDeviceToHost, b->stream));
     CK(cudaStreamSynchronize(b->stream));

@@ -1581,17 +1581,16 @@ int mgp_fill_sine_modes(mgp_solver* s, int n_modes, const double* amp, const dou
         m.wz[i] = kz[i] * pi / L[2];
     }
     DeviceGuard guard(s->device);
-    SineModes* dm = nullptr;
-    CK(cudaMallocAsync((void**)&dm, sizeof(SineModes), s->stream));
-    cudaError_t e = cudaMemcpyAsync(dm, &m, sizeof(SineModes), cudaMemcpyHostToDevice, s->stream);
     LevelState& L0 = s->lv[0];
-    const long long n = (long long)L0.G.nx * L0.G.ny * L0.G.nz;
-    if (e == cudaSuccess) {
-        k_fill_sine<<<grid_1d(s, n), kThreads, 0, s->stream>>>((double*)L0.f, L0.G, L0.h, dm);
-        e = cudaGetLastError();
-        s->launches++;
-    }
-    cudaFreeAsync(dm, s->stream);
+    const Geom& G = L0.G;
+    dim3 grid((G.nz + 31) / 32, (G.ny + 7) / 8, 1);
+    const int tiles = (int)(grid.x * grid.y);
+    const int chunks = std::max(1, std::min(G.nx, (sm_count(s->device) * 8 + tiles - 1) / tiles));
+    const int ichunk = (G.nx + chunks - 1) / chunks;
+    grid.z = (G.nx + ichunk - 1) / ichunk;
+    k_fill_sine<<<grid, kThreads, 0, s->stream>>>((double*)L0.f, G, L0.h, m, ichunk);
+    cudaError_t e = cudaGetLastError();
+    s->launches++;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return fail(MGP_ERR_CUDA, "sine-mode fill: %s", cudaGetErrorString(e));
     return MGP_OK;

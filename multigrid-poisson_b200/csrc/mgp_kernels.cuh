@@ -1248,17 +1248,32 @@ struct SineModes {
     double amp[64], wx[64], wy[64], wz[64];  // wx = kx*pi/Lx etc.
 };
 
-__global__ void __launch_bounds__(256) k_fill_sine(double* f, Geom G, double h, const SineModes* __restrict__ m) {
-    const long long n = (long long)G.nx * G.ny * G.nz;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t % G.nz);
-        const long long q = t / G.nz;
-        const int j = (int)(q % G.ny);
-        const int i = (int)(q / G.ny);
-        const double x = i * h, y = j * h, z = k * h;
-        double acc = 0.0;
-        for (int s = 0; s < m->n; s++) acc += m->amp[s] * sin(m->wx[s] * x) * sin(m->wy[s] * y) * sin(m->wz[s] * z);
-        f[(long long)i * G.sx + (long long)j * G.sy + k] = acc;
+// f(i,j,k) = sum_s amp[s] sin(wx[s] x) sin(wy[s] y) sin(wz[s] z), (x,y,z) = (i,j,k)*h.  The modes
+// are separable, so a block (a tile of 32 k by 8 j, marching a range of planes i) evaluates the
+// sines of its k and j values once into shared memory and those of each plane once; every
+// point then sums the same products in the same order as a direct evaluation would.
+__global__ void __launch_bounds__(256) k_fill_sine(double* f, Geom G, double h, const SineModes m, int ichunk) {
+    __shared__ double sz[64][32], sy[64][8], sx[64];
+    const int tk = threadIdx.x & 31, tj = threadIdx.x >> 5;
+    const int k = blockIdx.x * 32 + tk, j = blockIdx.y * 8 + tj;
+    for (int q = threadIdx.x; q < m.n * 32; q += 256) {
+        const int s = q >> 5, kk = blockIdx.x * 32 + (q & 31);
+        sz[s][q & 31] = sin(m.wz[s] * (kk * h));
+    }
+    for (int q = threadIdx.x; q < m.n * 8; q += 256) {
+        const int s = q >> 3, jj = blockIdx.y * 8 + (q & 7);
+        sy[s][q & 7] = sin(m.wy[s] * (jj * h));
+    }
+    const int i0 = blockIdx.z * ichunk, i1 = min(G.nx, i0 + ichunk);
+    for (int i = i0; i < i1; i++) {
+        __syncthreads();  // tables ready; the previous plane's sx no longer read
+        if (threadIdx.x < m.n) sx[threadIdx.x] = sin(m.wx[threadIdx.x] * (i * h));
+        __syncthreads();
+        if (k < G.nz && j < G.ny) {
+            double acc = 0.0;
+            for (int s = 0; s < m.n; s++) acc += m.amp[s] * sx[s] * sy[s][tj] * sz[s][tk];
+            f[(long long)i * G.sx + (long long)j * G.sy + k] = acc;
+        }
     }
 }
 

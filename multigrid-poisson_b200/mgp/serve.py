@@ -114,15 +114,18 @@ class Server:
         self.steps = 0
         self.batch_sizes = []
         self._landing = None  # page-locked download buffer, grown to the largest solution
+        self._free = None     # device bytes left for admissions in the current tick
 
     def close(self):
         self.batch.close()
 
     def _admit(self, req: Request, now: float) -> bool:
         need = self.batch.problem_bytes(req.dims, req.levels, req.h, req.bc)
-        free, _ = self.batch.mem_info()
-        if free - need < self.reserve:
+        if self._free is None:  # device memory is queried once per server tick
+            self._free, _ = self.batch.mem_info()
+        if self._free - need < self.reserve:
             return False
+        self._free -= need
         pid = self.batch.add(req.dims, req.levels, req.h, req.bc)
         s = self.batch.problem(pid)
         s.fill_sine_modes(req.amp, req.kx, req.ky, req.kz, req.lengths)
@@ -167,6 +170,7 @@ class Server:
             now = clock() - t0
             while pending and pending[0].arrival * time_scale <= now:
                 waiting.append(pending.popleft())
+            self._free = None
             while waiting and len(self._active) < self.max_batch and self._admit(waiting[0], now):
                 waiting.popleft()
             if not self._active:

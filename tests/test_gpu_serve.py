@@ -50,3 +50,22 @@ def test_admission_respects_device_memory(mgp_mod, gpu_ready):
     srv.close()
     assert stats["converged"] == len(reqs)
     assert stats["max_batch_seen"] <= 2
+
+
+def test_sine_mode_rhs_matches_its_formula(mgp_mod, gpu_ready):
+    """The device-side right-hand side of a served request is the sum of its sine modes."""
+    from mgp import serve
+
+    req = serve.make_request(3, 0.0, seed=11, kmin=4, kmax=6)
+    s = mgp_mod.Solver(req.dims, req.levels, req.h, req.bc, mgp_mod.FULLWEIGHTING, mgp_mod.GAUSSSEIDEL, mgp_mod.F64)
+    s.fill_sine_modes(req.amp, req.kx, req.ky, req.kz, req.lengths)
+    f = s.download("f", 0)[s.level[0].interior]
+    s.close()
+    x, y, z = (np.arange(n) * req.h for n in req.dims)
+    L = req.lengths
+    want = np.zeros(req.dims)
+    for a, kx, ky, kz in zip(req.amp, req.kx, req.ky, req.kz):
+        want += a * np.sin(kx * np.pi / L[0] * x)[:, None, None] * np.sin(ky * np.pi / L[1] * y)[None, :, None] * \
+            np.sin(kz * np.pi / L[2] * z)[None, None, :]
+    # tolerance: libm and CUDA sin may differ in the last bit
+    assert np.allclose(f, want, rtol=1e-12, atol=1e-13)
