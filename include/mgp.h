@@ -265,6 +265,10 @@ int mgp_batch_kernel_launches(const mgp_batch* b, int64_t* per_step);
  * stream's order, and give their memory back to it on removal).  No counterpart in the
  * reference, which has no batching. */
 int mgp_batch_mem_info(mgp_batch* b, size_t* free_bytes, size_t* total_bytes);
+/* Reserve `bytes` of device memory in the batch's memory pool up front (allocated once and
+ * returned to the pool, which keeps it): problems added later are carved out of it without
+ * the pool growing while the batch is serving.  No counterpart in the reference. */
+int mgp_batch_reserve(mgp_batch* b, size_t bytes);
 
 /* Free and total device memory (cudaMemGetInfo) of `device`, for admission control. */
 int mgp_mem_info(int device, size_t* free_bytes, size_t* total_bytes);

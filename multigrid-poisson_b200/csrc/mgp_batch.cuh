@@ -742,6 +742,20 @@ int mgp_batch_kernel_launches(const mgp_batch* b, int64_t* per_step) {
     return MGP_OK;
 }
 
+int mgp_batch_reserve(mgp_batch* b, size_t bytes) {
+    if (!b) return fail(MGP_ERR_INVALID_ARG, "null batch");
+    if (!bytes) return MGP_OK;
+    DeviceGuard guard(b->device);
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, b->pool, b->stream);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "reserving %zu bytes: %s", bytes,
+                    cudaGetErrorString(e));
+    CK(cudaFreeAsync(p, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return MGP_OK;
+}
+
 int mgp_batch_mem_info(mgp_batch* b, size_t* free_bytes, size_t* total_bytes) {
     if (!b || !free_bytes || !total_bytes) return fail(MGP_ERR_INVALID_ARG, "null argument");
     DeviceGuard guard(b->device);

@@ -133,6 +133,7 @@ def lib():
         L.mgp_batch_solve.argtypes = [vp, dbl, i64, ctypes.POINTER(i64)]
         L.mgp_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(i64)]
         L.mgp_batch_mem_info.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+        L.mgp_batch_reserve.argtypes = [vp, ctypes.c_size_t]
         L.mgp_mem_info.argtypes = [i32, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
         dp = ctypes.POINTER(dbl)
         L.mgp_fill_sine_modes.argtypes = [vp, i32, dp, dp, dp, dp, dp]
@@ -499,6 +500,10 @@ class Batch:
         k = ctypes.c_int64()
         _check(lib().mgp_batch_kernel_launches(self._h, ctypes.byref(k)))
         return k.value
+
+    def reserve(self, nbytes: int):
+        """Reserve nbytes of device memory in the batch's pool up front (kept by the pool)."""
+        _check(lib().mgp_batch_reserve(self._h, int(nbytes)))
 
     def mem_info(self):
         """(free, total) device bytes available to this batch: the device's free memory plus

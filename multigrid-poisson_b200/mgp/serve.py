@@ -66,8 +66,9 @@ def make_request(rid: int, arrival: float, seed: int, kmin=5, kmax=9, tol=1e-8, 
     """Box sides 2^k+1 (k uniform in [kmin, kmax] independently per axis, z at most kmax_z),
     levels down to a
     5-point coarsest side, boundary kind uniform over Dirichlet / Neumann (the reference's
-    default {N,N,N,N,D,D}) / mixed (random per face, top and bottom alike so that the
-    red-black colouring stays well defined), zero boundary data, and a right-hand side of 8
+    default {N,N,N,N,D,D}) / mixed (random per face pair: north with south, east, west, top
+    with bottom, so that the red-black colouring is a true checkerboard), zero boundary
+    data, and a right-hand side of 8
     sine modes with wavenumbers uniform in 1..8 and N(0,1) amplitudes from the request's seed."""
     rng = rng or np.random.default_rng((seed, rid, 1))
     k = rng.integers(kmin, kmax + 1, size=3)
@@ -82,7 +83,10 @@ def make_request(rid: int, arrival: float, seed: int, kmin=5, kmax=9, tol=1e-8, 
         bc = (1, 1, 1, 1, 0, 0)
     else:
         ns, ew = rng.integers(0, 2, size=4), int(rng.integers(0, 2))
-        bc = (int(ns[0]), int(ns[1]), int(ns[2]), int(ns[3]), ew, ew)
+        # north/south alike and top/bottom alike keep the padded y and z extents odd: the
+        # reference's red-black colouring is then a true checkerboard (its degenerate
+        # layouts, swept column by column, are left out of the served mix)
+        bc = (int(ns[0]), int(ns[0]), int(ns[2]), int(ns[3]), ew, ew)
     mr = np.random.default_rng((seed, rid, 2))
     return Request(rid, arrival, dims, levels, 1.0 / (max(dims) - 1), bc, kind, mr.standard_normal(8),
                    mr.integers(1, 9, size=8).astype(np.float64), mr.integers(1, 9, size=8).astype(np.float64),
@@ -102,9 +106,17 @@ def make_stream(n: int, rate: float, seed: int = 0, **kw) -> list:
 
 class Server:
     def __init__(self, inner=F32, max_batch=64, reserve_bytes=4 << 30, device=0, max_steps=200,
-                 keep_solutions=False, nsmooth=2, digest=False):
+                 keep_solutions=False, nsmooth=2, digest=False, pool_bytes=None):
+        """pool_bytes: device memory the batch's pool takes up front (default: what
+        cudaMemGetInfo reports free, less reserve_bytes and 1 GiB), so that admitting and
+        retiring requests never grows or shrinks it; 0 lets the pool grow on demand."""
         self.batch = Batch(FULLWEIGHTING, GAUSSSEIDEL, inner, "Fcycle", nsmooth, max_problems=max_batch,
                            device=device)
+        if pool_bytes is None:
+            free, _ = self.batch.mem_info()
+            pool_bytes = max(0, free - reserve_bytes - (1 << 30))
+        if pool_bytes:
+            self.batch.reserve(pool_bytes)
         self.max_batch = max_batch
         self.reserve = reserve_bytes
         self.device = device

@@ -27,7 +27,7 @@ def test_served_results_equal_alone_and_in_mix(mgp_mod, gpu_ready, inner):
     for r in reqs:
         assert r.rel_res < r.tol
         alone = serve.make_stream(len(reqs), rate=2000.0, seed=7, kmin=4, kmax=6, tol=1e-8)[r.rid]
-        s1 = serve.Server(inner=dt, max_batch=1, keep_solutions=True)
+        s1 = serve.Server(inner=dt, max_batch=1, keep_solutions=True, pool_bytes=0)
         s1.run([alone])
         s1.close()
         assert alone.iterations == r.iterations
