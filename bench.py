@@ -46,6 +46,11 @@ BC = (1, 1, 1, 1, 0, 0)  # N S E W T B requested
 NSMOOTH = 2
 E2E_CYCLES = 4
 REF_ARM_CYCLES = 30   # timed cycles of the reference arm (a bounded sample)
+# DRAM bytes (read + write) of one level-0 Jacobi sweep launch at this size, from an ncu capture
+# of two launches: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#   --clock-control none -k regex:k_stencil -c 2 python bench.py --kernels --steps 1
+# (408.6 MB and 404.0 MB; algorithmic 408.2 MB).
+JACOBI_SWEEP_DRAM_BYTES = 406.3e6
 CPU_BASELINE_CYCLES = 8
 NDOF = DIMS[0] * DIMS[1] * DIMS[2]
 METRIC = "F-cycle fine-grid DOF/s (FP64, 513x257x129)"
@@ -608,7 +613,8 @@ def main():
                 "step": f"to_device + {E2E_CYCLES}-cycle solve + to_host", "ms_per_request": 1e3 * e2e_sec},
         "roofline": {"bound": "hbm", "kernel": "k_stencil<double,OP_JACOBI> level 0", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": None, "algorithmic_bytes_per_launch": kbytes, "launch_us": ksec * 1e6},
+                     "traffic": JACOBI_SWEEP_DRAM_BYTES, "traffic_source": "ncu dram__bytes_read+write, 2 launches",
+                     "algorithmic_bytes_per_launch": kbytes, "launch_us": ksec * 1e6},
         "cycle_roofline": {"model_bytes_per_cycle": cyc_bytes, "achieved": cyc_achieved, "peak": peak,
                            "unit": "GB/s", "frac": cyc_achieved / peak, "ms_per_cycle": 1e3 * sec / args.steps},
         "gpu_launches": int(st.kernel_launches),
