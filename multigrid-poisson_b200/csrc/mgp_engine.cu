@@ -85,6 +85,7 @@ struct LevelState {
     void* face[6] = {};
     int64_t face_shape[6][3];
     int cur = 0;            // index of the buffer that is "u" (Domain::swap_u, domain.h:311-316)
+    bool first_done = false;  // the set-up of the finer level already did this level's first sweep
     bool gs_column = false; // padded y extent even: colour depends on (j,k) only; whole columns
     mgp_level_info info;    // host (reference) layout
     // TMA-fed stencil sweeps (large levels): tensor maps of both u buffers and of f
@@ -429,17 +430,23 @@ template <typename T>
 int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth) {
     // Relaxation<T>::relax (include/relaxation.h:19-94)
     LevelState& L = s->lv[l];
+    // first_done: the coarse-grid set-up that just zeroed this level also wrote its first sweep
+    const bool skip_first = L.first_done;
+    L.first_done = false;
     if (s->desc.relaxation == MGP_JACOBI) {
         for (int64_t it = 0; it < nsmooth; it++) {
             L.cur ^= 1;  // swap_u: the previous iterate becomes the source
+            if (it == 0 && skip_first) continue;
             CKS((launch_stencil<T, OP_JACOBI>(s, l, uprev_ptr(s, l), u_ptr(s, l), (T)omega, 0, nullptr)));
         }
     } else {
         for (int64_t it = 0; it < 2 * nsmooth; it++) {
             const int colour = s->gs_alternate ? 0 : 1;
             void* u = u_ptr(s, l);
-            if (L.gs_column) CKS((launch_stencil<T, OP_GS_COLUMN>(s, l, u, u, (T)omega, colour, nullptr)));
-            else CKS((launch_stencil<T, OP_GS>(s, l, u, u, (T)omega, colour, nullptr)));
+            if (!(it == 0 && skip_first)) {
+                if (L.gs_column) CKS((launch_stencil<T, OP_GS_COLUMN>(s, l, u, u, (T)omega, colour, nullptr)));
+                else CKS((launch_stencil<T, OP_GS>(s, l, u, u, (T)omega, colour, nullptr)));
+            }
             s->gs_alternate = !s->gs_alternate;
         }
     }
@@ -476,14 +483,38 @@ RestrictArgs<T> restrict_args(mgp_solver* s, int l, bool zero_coarse_u, long lon
     a.vo = level_view(C);
     a.zero_u = zero_coarse_u ? (T*)u_ptr(s, l + 1) : nullptr;
     a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
+    a.fs = FirstSweep<T>{};
     *npts = (long long)C.G.nx * C.G.ny * C.G.nz;
     return a;
 }
 
+// The first sweep of level l+1, written by the set-up of level l (it runs right before that
+// level's relaxation in every cycle), with the constants launch_stencil would form.  Off for
+// column-ordered Gauss-Seidel (a sequential sweep) and without smoothing.
 template <typename T>
-int restrict_t(mgp_solver* s, int l, bool zero_coarse_u) {
+FirstSweep<T> first_sweep_of(mgp_solver* s, int l, double omega, int64_t ns) {
+    FirstSweep<T> w{};
+    LevelState& C = s->lv[l + 1];
+    if (ns < 1 || C.gs_column) return w;
+    w.on = 1;
+    w.gs = s->desc.relaxation == MGP_GAUSSSEIDEL;
+    w.colour = s->gs_alternate ? 0 : 1;
+    w.uw = w.gs ? (T*)u_ptr(s, l + 1) : (T*)C.ubuf[C.cur ^ 1];
+    for (int f = 0; f < 6; f++) w.gc[f] = (const T*)C.face[f];
+    w.G = C.G;
+    const T om = (T)omega;
+    w.one_omega = (T)(1.0 - om);
+    w.omega_sixth = (T)(om / 6.0);
+    w.hsq = (T)(C.h * C.h);
+    w.two_h = (T)(2.0 * C.h);
+    return w;
+}
+
+template <typename T>
+int restrict_t(mgp_solver* s, int l, bool zero_coarse_u, const FirstSweep<T>& w = FirstSweep<T>{}) {
     long long n = 0;
     RestrictArgs<T> a = restrict_args<T>(s, l, zero_coarse_u, &n);
+    a.fs = w;
     const LevelState& C = s->lv[l + 1];
     return launch_k(s, k_restrict<T>, dim3((C.G.ny * C.G.nz + kThreads - 1) / kThreads, C.G.nx), dim3(kThreads), 0, a);
 }
@@ -562,11 +593,12 @@ BcRestrictArgs<T> bc_args(mgp_solver* s, int l, bool* any) {
 // Coarse-grid correction set-up (vcycle.h:34-76, fcycle.h:130-172) in one launch:
 // residual(l) -> restrict -> u_{l+1}.init_zero(), plus the Neumann face restriction.
 template <typename T>
-int coarse_setup_fused_t(mgp_solver* s, int l) {
+int coarse_setup_fused_t(mgp_solver* s, int l, const FirstSweep<T>& w) {
     LevelState& F = s->lv[l];
     LevelState& C = s->lv[l + 1];
     constexpr int V = VecT<T>::V;
     RRArgs<T> a;
+    a.fs = w;
     a.Gf = F.G;
     a.Gc = C.G;
     a.u = (const T*)u_ptr(s, l);
@@ -645,13 +677,17 @@ int coarse_setup_fused_t(mgp_solver* s, int l) {
 constexpr long long kFusedSetupMaxPoints = 1ll << 20;
 
 template <typename T>
-int coarse_setup_t(mgp_solver* s, int l) {
+int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns) {
     const Geom& G = s->lv[l].G;
-    if ((s->desc.flags & MGP_FLAG_FUSED_SETUP) || (long long)G.nx * G.ny * G.nz <= kFusedSetupMaxPoints)
-        return coarse_setup_fused_t<T>(s, l);
-    CKS(residual_t<T>(s, l, nullptr));
-    CKS(restrict_t<T>(s, l, /*zero_coarse_u=*/true));
-    CKS(restrict_bc_t<T>(s, l));
+    const FirstSweep<T> w = first_sweep_of<T>(s, l, omega, ns);
+    if ((s->desc.flags & MGP_FLAG_FUSED_SETUP) || (long long)G.nx * G.ny * G.nz <= kFusedSetupMaxPoints) {
+        CKS(coarse_setup_fused_t<T>(s, l, w));
+    } else {
+        CKS(residual_t<T>(s, l, nullptr));
+        CKS(restrict_bc_t<T>(s, l));  // before the restriction: the first sweep reads the coarse faces
+        CKS(restrict_t<T>(s, l, /*zero_coarse_u=*/true, w));
+    }
+    s->lv[l + 1].first_done = w.on != 0;
     return MGP_OK;
 }
 
@@ -660,7 +696,7 @@ int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
     // Vcycle<T> (include/vcycle.h:14-98)
     CKS(relax_t<T>(s, l, omega, ns));
     if (l >= s->levels - 1) return MGP_OK;
-    CKS(coarse_setup_t<T>(s, l));
+    CKS(coarse_setup_t<T>(s, l, omega, ns));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
     CKS((prolong_t<T, true>(s, l)));
     CKS(relax_t<T>(s, l, omega, ns));
@@ -671,7 +707,7 @@ template <typename T>
 int fcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
     // Fcycle<T> (include/fcycle.h:13-97)
     CKS(relax_t<T>(s, l, omega, ns));
-    CKS(coarse_setup_t<T>(s, l));
+    CKS(coarse_setup_t<T>(s, l, omega, ns));
     if (l < s->levels - 2) CKS(fcycle_t<T>(s, l + 1, omega, ns));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
     CKS((prolong_t<T, true>(s, l)));

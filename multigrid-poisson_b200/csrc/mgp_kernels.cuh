@@ -437,6 +437,25 @@ __device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j,
 }
 
 template <typename T>
+struct RestrictArgs;
+
+// The first relaxation of a coarse level right after the set-up zeroed its u
+// (include/vcycle.h:43-50 then relaxation.h:19-94): every value it reads is the zero just
+// written or a Neumann ghost (sign*2h)*g + 0, so it is a pointwise function of the restricted
+// right-hand side and the coarse face data, and the restriction writes it directly.  The
+// expression is the sweep's own, operand for operand, with the zeros in place.
+template <typename T>
+struct FirstSweep {
+    int on;          // 0: the set-up only zeroes the coarse u
+    int gs;          // red-black half-sweep in place (1) or Jacobi into `uw` (0)
+    int colour;      // red-black colour of the half-sweep
+    T* uw;           // Jacobi: the buffer the sweep writes (the zeroed one is the source)
+    const T* gc[6];  // coarse face data, when already restricted (else formed inline)
+    Geom G;          // coarse level (relaxation bounds, colour offset)
+    T one_omega, omega_sixth, hsq, two_h;
+};
+
+template <typename T>
 struct RestrictArgs {
     const T* in;
     View vi;
@@ -444,7 +463,52 @@ struct RestrictArgs {
     View vo;
     T* zero_u;  // coarse u to zero alongside (nullptr: none)
     int fw;
+    FirstSweep<T> fs;
 };
+
+// Offset of face-array indices (fi, fj, fk) in a dense face array of a level with ny x nz
+// points per i-plane: west/east (1,ny,nz), south/north (nx,1,nz), bottom/top (nx,ny,1).
+__device__ __forceinline__ long long face_offset(int fc, int ny, int nz, int fi, int fj, int fk) {
+    if (fc == F_WEST || fc == F_EAST) return (long long)fj * nz + fk;
+    if (fc == F_SOUTH || fc == F_NORTH) return (long long)fi * nz + fk;
+    return (long long)fi * ny + fj;
+}
+
+// Value of the first sweep at coarse point (i,j,k) inside the relaxation bounds; g(face, fi,
+// fj, fk) gives the coarse face value at face-array indices (fi, fj, fk).
+template <typename T, typename G>
+__device__ __forceinline__ T first_sweep_value(const FirstSweep<T>& w, T fc, int i, int j, int k, G g) {
+    const Geom& C = w.G;
+    const T z = T(0), two_h = w.two_h, m2h = -w.two_h;
+    const T vm = i == 0 ? m2h * g(F_WEST, 0, j, k) + z : z;            // -2h*gW + u(1)
+    const T vp = i == C.nx - 1 ? two_h * g(F_EAST, 0, j, k) + z : z;    // 2h*gE + u(nx-2)
+    const T ym = j == 0 ? m2h * g(F_SOUTH, i, 0, k) + z : z;
+    const T yp = j == C.ny - 1 ? two_h * g(F_NORTH, i, 0, k) + z : z;
+    const T zm = k == 0 ? m2h * g(F_BOTTOM, i, j, 0) + z : z;
+    const T zp = k == C.nz - 1 ? two_h * g(F_TOP, i, j, 0) + z : z;
+    const T sum = vm + vp + ym + yp + zm + zp;
+    return w.one_omega * z + w.omega_sixth * (sum - w.hsq * fc);
+}
+
+// The set-up's coarse write at offset o of coarse point (i,j,k): u = 0, and the first sweep
+// where it is enabled.
+template <typename T, typename G>
+__device__ __forceinline__ void coarse_u_write(const FirstSweep<T>& w, T* zero_u, long long o, T fc, int i, int j,
+                                               int k, G g) {
+    if (!w.on) {
+        zero_u[o] = T(0);
+        return;
+    }
+    const Geom& C = w.G;
+    const bool inside = i >= C.x0 && i < C.x1 && j >= C.y0 && j < C.y1 && k >= C.z0 && k < C.z1;
+    if (w.gs) {
+        const bool act = inside && ((i + j + k + C.poff) & 1) == w.colour;
+        zero_u[o] = act ? first_sweep_value(w, fc, i, j, k, g) : T(0);
+    } else {
+        zero_u[o] = T(0);
+        if (inside) w.uw[o] = first_sweep_value(w, fc, i, j, k, g);
+    }
+}
 
 // Coarse plane `i` (the tile's y index), coarse points j*n[2]+k = bx*256 + thread of it.
 template <typename T>
@@ -459,7 +523,12 @@ __device__ __forceinline__ void restrict_tile(const RestrictArgs<T>& a, const in
     if (a.fw) v = fw_point(a.in, a.vi, i, j, k);
     else v = ldg(a.in + (2 * i) * a.vi.s0 + (2 * j) * a.vi.s1 + 2 * k);  // injection.h:63
     a.out[o] = v;
-    if (a.zero_u) a.zero_u[o] = T(0);
+    if (a.zero_u) {
+        auto g = [&](int fc, int fi, int fj, int fk) -> T {  // coarse faces restricted before this launch
+            return ldg(a.fs.gc[fc] + face_offset(fc, vo.n[1], vo.n[2], fi, fj, fk));
+        };
+        coarse_u_write(a.fs, a.zero_u, o, v, i, j, k, g);
+    }
 }
 
 // grid: ((n[1]*n[2] + 255)/256, n[0]) of the coarse view
@@ -483,11 +552,9 @@ struct BcRestrictArgs {
     bool fw;
 };
 
-// Work of one face: thread `tid` of `nthr` cooperating threads.
+// Neumann::restrict_to at one point (i,j,k) of face fc's coarse array (face-array indices).
 template <typename T>
-__device__ __forceinline__ void bc_restrict_face(const BcRestrictArgs<T>& a, int fc, long long tid, long long nthr) {
-    const View vo = a.vc[fc];
-    const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
+__device__ __forceinline__ T bc_restrict_value(const BcRestrictArgs<T>& a, int fc, int i, int j, int k) {
     const int nxf = a.Gf.nx, nyf = a.Gf.ny, nzf = a.Gf.nz;
     int offx = 0, offy = 0, offz = 0, ii = 0, jj = 0, kk = 0, iii = 0, jjj = 0, kkk = 0;
     T c1 = T(-3.0 / 2.0), c2 = T(2.0), c3 = T(-0.5);
@@ -504,17 +571,25 @@ __device__ __forceinline__ void bc_restrict_face(const BcRestrictArgs<T>& a, int
         c2 = T(-2.0);
         c1 = T(3.0 / 2.0);
     }
+    T g = a.fw ? fw_point(a.gf[fc], a.vf[fc], i, j, k)
+               : ldg(a.gf[fc] + (2 * i) * a.vf[fc].s0 + (2 * j) * a.vf[fc].s1 + 2 * k);
+    const int x = 2 * (i + offx), y = 2 * (j + offy), z = 2 * (k + offz);
+    auto U = [&](int xx, int yy, int zz) -> T { return ldg(a.u + xx * a.Gf.sx + yy * a.Gf.sy + zz); };
+    g -= (c1 * U(x, y, z) + c2 * U(x + ii, y + jj, z + kk) + c3 * U(x + iii, y + jjj, z + kkk)) / a.h;
+    return g;
+}
+
+// Work of one face: thread `tid` of `nthr` cooperating threads.
+template <typename T>
+__device__ __forceinline__ void bc_restrict_face(const BcRestrictArgs<T>& a, int fc, long long tid, long long nthr) {
+    const View vo = a.vc[fc];
+    const long long n = (long long)vo.n[0] * vo.n[1] * vo.n[2];
     for (long long t = tid; t < n; t += nthr) {
         const int k = (int)(t % vo.n[2]);
         const long long q = t / vo.n[2];
         const int j = (int)(q % vo.n[1]);
         const int i = (int)(q / vo.n[1]);
-        T g = a.fw ? fw_point(a.gf[fc], a.vf[fc], i, j, k)
-                   : ldg(a.gf[fc] + (2 * i) * a.vf[fc].s0 + (2 * j) * a.vf[fc].s1 + 2 * k);
-        const int x = 2 * (i + offx), y = 2 * (j + offy), z = 2 * (k + offz);
-        auto U = [&](int xx, int yy, int zz) -> T { return ldg(a.u + xx * a.Gf.sx + yy * a.Gf.sy + zz); };
-        g -= (c1 * U(x, y, z) + c2 * U(x + ii, y + jj, z + kk) + c3 * U(x + iii, y + jjj, z + kkk)) / a.h;
-        a.gc[fc][i * vo.s0 + j * vo.s1 + k] = g;
+        a.gc[fc][i * vo.s0 + j * vo.s1 + k] = bc_restrict_value<T>(a, fc, i, j, k);
     }
 }
 
@@ -570,21 +645,32 @@ struct RRArgs {
     int tjc, tkc, ci;
     int tiles_j, tiles_k, main_blocks, bc_blocks_per_face;
     BcRestrictArgs<T> bc;
+    FirstSweep<T> fs;
 };
+
+// The set-up's write of coarse u at (I, J, K): zero, or the first sweep, whose Neumann ghosts
+// take the coarse face values formed here (the face-restriction blocks of the same launch
+// write the same values to the face arrays).
+template <typename T>
+__device__ __forceinline__ void rr_coarse_u(const RRArgs<T>& a, long long oo, T fc, int I, int J, int K) {
+    auto g = [&](int face, int fi, int fj, int fk) -> T { return bc_restrict_value<T>(a.bc, face, fi, fj, fk); };
+    coarse_u_write(a.fs, a.uc, oo, fc, I, J, K, g);
+}
 
 // The share of fine plane q (residual tile P, rows pre-multiplied by the tile row width) in
 // the coarse point's restriction: Injection at the coarse plane q/2, or FullWeighting's
 // running sums, i-major with weights (1,2,1 | 2,4,2 | 1,2,1), doubled on the ii plane.
 template <typename T>
 __device__ __forceinline__ void rr_accumulate(const T* P, int q, const RRArgs<T>& a, int I0, int I1, int nxf, int rm,
-                                              int rj, int rp, int cm, int ck, int cp, long long o, double& s_m,
-                                              double& s_0, double& s_p) {
+                                              int rj, int rp, int cm, int ck, int cp, long long o, int J, int K,
+                                              double& s_m, double& s_0, double& s_p) {
     const Geom& Gc = a.Gc;
     if (!a.fw) {
         if (!(q & 1) && (q >> 1) >= I0 && (q >> 1) < I1) {  // injection.h:63
             const long long oo = (long long)(q >> 1) * Gc.sx + o;
-            a.fc[oo] = P[rj + ck];
-            a.uc[oo] = T(0);
+            const T v = P[rj + ck];
+            a.fc[oo] = v;
+            rr_coarse_u(a, oo, v, q >> 1, J, K);
         }
         return;
     }
@@ -612,8 +698,9 @@ __device__ __forceinline__ void rr_accumulate(const T* P, int q, const RRArgs<T>
         tmp = (T)((double)tmp + s_0);
         tmp = (T)((double)tmp + s_p);
         const long long oo = (long long)I * Gc.sx + o;
-        a.fc[oo] = (T)((double)tmp / 64.0);
-        a.uc[oo] = T(0);
+        const T v = (T)((double)tmp / 64.0);
+        a.fc[oo] = v;
+        rr_coarse_u(a, oo, v, I, J, K);
     };
     if (q & 1) {
         const int Ip = (q - 1) >> 1, Im = (q + 1) >> 1;
@@ -872,11 +959,12 @@ __global__ void __launch_bounds__(384, 2) k_resid_restrict(RRArgs<T> a) {
             // the coarse points' share of fine plane i-1, whose residual tile is complete
             const int q = i - 1;
             const T* P = rtile + (q & 1) * (R * TW);
-            rr_accumulate(P, q, a, I0, I1, Gf.nx, rm, rj, rp, cm, ck, cp, o, s_m, s_0, s_p);
+            rr_accumulate(P, q, a, I0, I1, Gf.nx, rm, rj, rp, cm, ck, cp, o, J, K, s_m, s_0, s_p);
         }
     }
     __syncthreads();
-    if (owner) rr_accumulate(rtile + (ib & 1) * (R * TW), ib, a, I0, I1, Gf.nx, rm, rj, rp, cm, ck, cp, o, s_m, s_0, s_p);
+    if (owner)
+        rr_accumulate(rtile + (ib & 1) * (R * TW), ib, a, I0, I1, Gf.nx, rm, rj, rp, cm, ck, cp, o, J, K, s_m, s_0, s_p);
     cp_async_wait<0>();
 }
 
