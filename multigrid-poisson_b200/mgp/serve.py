@@ -126,18 +126,25 @@ class Server:
         self.steps = 0
         self.batch_sizes = []
         self._landing = None  # page-locked download buffer, grown to the largest solution
-        self._free = None     # device bytes left for admissions in the current tick
+        self._free = None     # device bytes left for admissions (the server's own count)
+        self._asked = False   # the device was asked in the current tick
+        self._need = {}       # bytes each resident request took
 
     def close(self):
         self.batch.close()
 
     def _admit(self, req: Request, now: float) -> bool:
         need = self.batch.problem_bytes(req.dims, req.levels, req.h, req.bc)
-        if self._free is None:  # device memory is queried once per server tick
+        # The server keeps its own count of free device memory: admissions take from it and
+        # retirements give back; the device is asked again (cudaMemGetInfo takes milliseconds)
+        # only when the count says no, at most once per tick.
+        if self._free is None or (self._free - need < self.reserve and not self._asked):
             self._free, _ = self.batch.mem_info()
+            self._asked = True
         if self._free - need < self.reserve:
             return False
         self._free -= need
+        self._need[req.rid] = need
         pid = self.batch.add(req.dims, req.levels, req.h, req.bc)
         s = self.batch.problem(pid)
         s.fill_sine_modes(req.amp, req.kx, req.ky, req.kz, req.lengths)
@@ -168,6 +175,8 @@ class Server:
         if self.keep:
             req.solution = u.copy()
         self.batch.remove(pid)
+        if self._free is not None:
+            self._free += self._need.pop(req.rid, 0)
         req.finished = now
 
     def run(self, requests, time_scale: float = 1.0, clock=time.perf_counter) -> dict:
@@ -182,7 +191,7 @@ class Server:
             now = clock() - t0
             while pending and pending[0].arrival * time_scale <= now:
                 waiting.append(pending.popleft())
-            self._free = None
+            self._asked = False
             while waiting and len(self._active) < self.max_batch and self._admit(waiting[0], now):
                 waiting.popleft()
             if not self._active:
