@@ -240,19 +240,9 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
         const unsigned full = (1u << V) - 1u;
         const int i0 = max(ia, G.x0);
         const int i1 = inr ? min(ib, G.x1) : i0;
-        if (NORM) {
-            // r outside the bounds keeps its value and still counts in the norm
-            // (infinity_norm runs over the whole shape, devicearray.h:221-237).  Here: the
-            // planes of the chunk outside the i bounds (all of them when this vector has no
-            // relaxed point); the unrelaxed points of relaxed planes are read in the march.
-            for (int i = ia; i < ib; i++) {
-                if (i >= i0 && i < i1) continue;
-                const T* rp = a.dst + (long long)i * G.sx + bjk;
-#pragma unroll
-                for (int e = 0; e < V; e++)
-                    if ((ins >> e) & 1u) mx = max(mx, abs_bits(rp[e]));
-            }
-        }
+        // NORM: the max over the points this march computes; the stored r outside the
+        // relaxation bounds, which also counts in the norm (infinity_norm runs over the whole
+        // shape, devicearray.h:221-237), is taken by k_norm_unrelaxed in the same reduction.
         if (i0 < i1) {
             // src may alias dst (in-place Gauss-Seidel): every value a thread reads belongs to
             // the colour this pass does not write, or to its own vector.
@@ -262,7 +252,7 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
             const T m2h = -two_h;
             T* su = &stage_u[0][threadIdx.x * V];
             T* sf = &stage_f[0][threadIdx.x * V];
-            const unsigned unr = NORM ? (ins & ~inr) : 0u;  // r staged at these elements
+            const unsigned unr = 0u;  // elements that would stage r in place of f (none)
             const T* rr = a.dst;
             constexpr int SS = 256 * V;  // stage stride
             // stage s holds u(i0+s+1) and f(i0+s)
@@ -301,11 +291,6 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                                                   : T(0);
                 }
                 lds_v(fc, sf + slot * SS);
-                if (NORM && unr) {  // stored r at the unrelaxed points of this plane
-#pragma unroll
-                    for (int e = 0; e < V; e++)
-                        if ((unr >> e) & 1u) mx = max(mx, abs_bits(fc[e]));
-                }
                 {  // refill this slot with plane i+kStages
                     const int q = i + kStages;
                     if (q < i1) {
@@ -1116,6 +1101,28 @@ __global__ void __launch_bounds__(256) k_add(T* u, const T* __restrict__ r, Geom
         const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
         u[p] = u[p] + ldg(r + p);
     }
+}
+
+// max |r| over the points outside the relaxation bounds (they keep their stored r), into the
+// same word as the residual march's max over the points inside: whole rows (i, j) outside the
+// bounds in i or j, and the k = 0 / nz-1 ends of the other rows when z has Dirichlet faces.
+// One thread per (i, j) row; grid: ((nx*ny + 255)/256).
+template <typename T>
+__global__ void __launch_bounds__(256) k_norm_unrelaxed(const T* __restrict__ r, Geom G, unsigned long long* out) {
+    pdl_begin();
+    const int t = blockIdx.x * 256 + (int)threadIdx.x;
+    unsigned long long mx = 0ull;
+    if (t < G.nx * G.ny) {
+        const int i = t / G.ny, j = t - (t / G.ny) * G.ny;
+        const T* row = r + (long long)i * G.sx + (long long)j * G.sy;
+        if (i < G.x0 || i >= G.x1 || j < G.y0 || j >= G.y1) {
+            for (int k = 0; k < G.nz; k++) mx = max(mx, abs_bits(ldg(row + k)));
+        } else {
+            for (int k = 0; k < G.z0; k++) mx = max(mx, abs_bits(ldg(row + k)));
+            for (int k = G.z1; k < G.nz; k++) mx = max(mx, abs_bits(ldg(row + k)));
+        }
+    }
+    block_max_to(mx, out);
 }
 
 // max |a| over the shape (DeviceArray::infinity_norm).  grid: ((ny*nz + 255)/256, chunks of
