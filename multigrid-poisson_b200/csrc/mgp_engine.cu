@@ -524,7 +524,9 @@ int restrict_t(mgp_solver* s, int l, bool zero_coarse_u, const FirstSweep<T>& w 
     RestrictArgs<T> a = restrict_args<T>(s, l, zero_coarse_u, &n);
     a.fs = w;
     const LevelState& C = s->lv[l + 1];
-    return launch_k(s, k_restrict<T>, dim3((C.G.ny * C.G.nz + kThreads - 1) / kThreads, C.G.nx), dim3(kThreads), 0, a);
+    const dim3 grid((C.G.ny * C.G.nz + kThreads - 1) / kThreads, C.G.nx);
+    if (a.zero_u && a.fs.on) return launch_k(s, k_restrict<T, true>, grid, dim3(kThreads), 0, a);
+    return launch_k(s, k_restrict<T, false>, grid, dim3(kThreads), 0, a);
 }
 
 template <typename T>
