@@ -73,6 +73,11 @@ typedef enum { MGP_CYCLE_RELAXATION = 0, MGP_CYCLE_V = 1, MGP_CYCLE_F = 2 } mgp_
 #define MGP_FLAG_REFINE_F64 32u /* iterative refinement, FP64 correction hierarchy */
 #define MGP_FLAG_TMA_SWEEPS 64u /* levels of >= 2^20 points sweep with the TMA-fed kernel (shared-memory plane
                                   rings filled by cp.async.bulk.tensor) instead of the per-thread cp.async march */
+#define MGP_FLAG_SWEEP_PAIRS 128u /* Jacobi relaxations of levels of >= 2^20 points make
+                                    consecutive sweeps two at a time in one pass (k_jacobi_pair:
+                                    same results, one more level-sized buffer per such level).  Off
+                                    by default: on B200 the pair still takes longer than two
+                                    single sweeps (513x257x129 FP64: 307-330 us against 2 x 85 us) */
 #define MGP_FLAG_FUSED_SETUP 8u /* cycles form the residual inside the restriction kernel (one
                                    launch, r never stored) on every level; without the flag only
                                    levels of at most 2^20 points do */

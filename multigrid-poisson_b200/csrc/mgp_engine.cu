@@ -29,6 +29,7 @@
 #include "mgp.h"
 #include "mgp_kernels.cuh"
 #include "mgp_stencil_tma.cuh"
+#include "mgp_sweep_pair.cuh"
 
 using namespace mgp;
 
@@ -93,6 +94,14 @@ struct LevelState {
     CUtensorMap map_u[2];
     CUtensorMap map_f;
     TmaTiling tiling;
+    // Paired Jacobi sweeps (large levels, k_jacobi_pair): a third level-sized buffer rotates
+    // with the two of the ping-pong pair; phys[] are the three allocations in their original
+    // order, whose arrangement over (ubuf[0], ubuf[1], spare) is part of the graph state.
+    bool pair = false;
+    void* spare = nullptr;
+    void* phys[3] = {nullptr, nullptr, nullptr};
+    int pair_tj = 0, pair_nvec = 0, pair_grid = 0;
+    size_t pair_smem = 0;
 };
 
 struct GraphEntry {
@@ -156,14 +165,42 @@ cudaError_t dev_zero(mgp_solver* s, void* p, size_t bytes) {
 }
 
 // ---- state helpers ----------------------------------------------------------------------
+// Graph state: bit 0 GaussSeidel::alternate, bit l+1 the current buffer of level l, and from
+// bit 32 four bits per level with paired sweeps: which allocations sit in ubuf[0] and ubuf[1]
+// (3*i0 + i1; the spare is the third).  Pairs are enabled on at most kPairMaxLevels levels of
+// solvers with at most 31 levels.
+constexpr int kPairMaxLevels = 8;
+int phys_index(const LevelState& L, const void* p) {
+    for (int i = 0; i < 3; i++)
+        if (L.phys[i] == p) return i;
+    return 0;
+}
 uint64_t state_bits(const mgp_solver* s) {
     uint64_t b = s->gs_alternate ? 1ull : 0ull;
     for (int l = 0; l < s->levels; l++) b |= (uint64_t)(s->lv[l].cur & 1) << (l + 1);
+    int pi = 0;
+    for (int l = 0; l < s->levels; l++) {
+        const LevelState& L = s->lv[l];
+        if (!L.pair) continue;
+        b |= (uint64_t)(3 * phys_index(L, L.ubuf[0]) + phys_index(L, L.ubuf[1])) << (32 + 4 * pi);
+        pi++;
+    }
     return b;
 }
 void set_state_bits(mgp_solver* s, uint64_t b) {
     s->gs_alternate = b & 1ull;
     for (int l = 0; l < s->levels; l++) s->lv[l].cur = (int)((b >> (l + 1)) & 1ull);
+    int pi = 0;
+    for (int l = 0; l < s->levels; l++) {
+        LevelState& L = s->lv[l];
+        if (!L.pair) continue;
+        const int code = (int)((b >> (32 + 4 * pi)) & 15ull);
+        const int i0 = code / 3, i1 = code % 3;
+        L.ubuf[0] = L.phys[i0];
+        L.ubuf[1] = L.phys[i1];
+        L.spare = L.phys[3 - i0 - i1];
+        pi++;
+    }
 }
 
 void* u_ptr(mgp_solver* s, int l) { return s->lv[l].ubuf[s->lv[l].cur]; }
@@ -386,6 +423,58 @@ int launch_stencil_tma(mgp_solver* s, int l, const StencilArgs<T>& a) {
     return launch_k_ordered(s, kernel, dim3(grid), dim3(threads), smem, mu, L.map_f, a, t, s->err_word);
 }
 
+// ---- paired Jacobi sweeps ----------------------------------------------------------------
+// With MGP_FLAG_SWEEP_PAIRS, levels of at least kPairMinPoints points (at least 3 per axis) make
+// consecutive Jacobi sweeps two at a time with k_jacobi_pair, unless the level sweeps with the
+// TMA-fed kernel or the solver is carved from a batch pool (the batch engine sweeps with its own
+// kernels).  Off by default: on B200 one pair launch of the 513x257x129 FP64 level takes
+// 307-330 us, two single sweeps 2 x 85 us.  A CTA covers tj+2 rows of nvec vectors (at most 1024 threads, tj >= 4);
+// tj is the largest that fits, evened out over the tiles of a plane.
+constexpr long long kPairMinPoints = 1ll << 20;
+constexpr size_t kPairMaxSmem = 200 * 1024;
+
+template <typename T>
+cudaError_t pair_prepare_level(mgp_solver* s, LevelState& L, int npair) {
+    constexpr int V = VecT<T>::V;
+    L.pair = false;
+    const Geom& G = L.G;
+    if (s->desc.relaxation != MGP_JACOBI || !(s->desc.flags & MGP_FLAG_SWEEP_PAIRS) || s->pool || L.tma ||
+        !L.ubuf[1] || s->levels > 31 || npair >= kPairMaxLevels || (long long)G.nx * G.ny * G.nz < kPairMinPoints ||
+        G.nx < 3 || G.ny < 3 || G.nz < 3)
+        return cudaSuccess;
+    const int nvec = (G.nz + V - 1) / V;
+    int tjmax = kPairMaxThreads / nvec - 2;
+    while (tjmax >= 4 && pair_smem_elems(tjmax, nvec, V) * sizeof(T) > kPairMaxSmem) tjmax--;
+    if (tjmax < 4) return cudaSuccess;
+    const int ntiles = (G.ny + tjmax - 1) / tjmax;
+    const int tj = (G.ny + ntiles - 1) / ntiles;
+    const size_t smem = pair_smem_elems(tj, nvec, V) * sizeof(T);
+    const int threads = (tj + 2) * nvec;
+    cudaError_t e = cudaFuncSetAttribute(k_jacobi_pair<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kPairMaxSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_jacobi_pair<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPairMaxSmem);
+    int per_sm = 0;
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_pair<T, true>, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaSuccess;
+    const long long work = (long long)ntiles * G.nx;
+    e = dev_alloc(s, &L.spare, L.elems * sizeof(T));
+    if (e == cudaSuccess) e = dev_zero(s, L.spare, L.elems * sizeof(T));
+    if (e != cudaSuccess) return e;
+    L.phys[0] = L.ubuf[0];
+    L.phys[1] = L.ubuf[1];
+    L.phys[2] = L.spare;
+    L.pair_tj = tj;
+    L.pair_nvec = nvec;
+    L.pair_smem = smem;
+    L.pair_grid = (int)std::min<long long>(work, (long long)sm_count(s->device) * per_sm);
+    L.pair = true;
+    return cudaSuccess;
+}
+
 // ---- stencil launches -------------------------------------------------------------------
 template <typename T, int OP>
 int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, int colour, unsigned long long* norm) {
@@ -426,18 +515,55 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     return launch_k(s, k_stencil<T, OP, false>, grid, dim3(kThreads), 0, a);
 }
 
+// Two Jacobi sweeps in one pass (k_jacobi_pair): u0 = u, u1 -> u_prev (write_u1), u2 -> the
+// spare buffer, which then becomes u; the old u becomes the spare.
 template <typename T>
-int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth) {
+int launch_pair(mgp_solver* s, int l, T omega, bool write_u1) {
+    LevelState& L = s->lv[l];
+    PairArgs<T> a;
+    a.G = L.G;
+    a.src = (const T*)u_ptr(s, l);
+    a.prev = (T*)uprev_ptr(s, l);
+    a.out = (T*)L.spare;
+    a.f = (const T*)L.f;
+    a.F = faces_of<T>(s, l);
+    // the constants of launch_stencil (jacobi.h:41-44, neumann.h:117)
+    a.two_h = (T)(2.0 * L.h);
+    a.hsq = (T)(L.h * L.h);
+    a.one_omega = (T)(1.0 - omega);
+    a.omega_sixth = (T)(omega / 6.0);
+    a.tj = L.pair_tj;
+    a.nvec = L.pair_nvec;
+    a.work = (long long)((L.G.ny + L.pair_tj - 1) / L.pair_tj) * L.G.nx;
+    const dim3 block((unsigned)((L.pair_tj + 2) * L.pair_nvec));
+    if (write_u1) CKS(launch_k(s, k_jacobi_pair<T, true>, dim3(L.pair_grid), block, L.pair_smem, a));
+    else CKS(launch_k(s, k_jacobi_pair<T, false>, dim3(L.pair_grid), block, L.pair_smem, a));
+    std::swap(L.ubuf[L.cur], L.spare);
+    return MGP_OK;
+}
+
+// later: another relaxation of this level follows in the same cycle before anything reads
+// u_prev (the pre-smoothing of a V- or F-cycle), so a sweep pair that ends the call may leave
+// u_prev's relaxed points stale: that later relaxation overwrites all of them.
+template <typename T>
+int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth, bool later = false) {
     // Relaxation<T>::relax (include/relaxation.h:19-94)
     LevelState& L = s->lv[l];
     // first_done: the coarse-grid set-up that just zeroed this level also wrote its first sweep
     const bool skip_first = L.first_done;
     L.first_done = false;
     if (s->desc.relaxation == MGP_JACOBI) {
-        for (int64_t it = 0; it < nsmooth; it++) {
+        for (int64_t it = 0; it < nsmooth;) {
+            if (L.pair && nsmooth - it >= 2 && !(it == 0 && skip_first)) {
+                // two swap_u's leave the current-buffer index as it was
+                CKS(launch_pair<T>(s, l, (T)omega, it + 2 >= nsmooth && !later));
+                it += 2;
+                continue;
+            }
             L.cur ^= 1;  // swap_u: the previous iterate becomes the source
-            if (it == 0 && skip_first) continue;
-            CKS((launch_stencil<T, OP_JACOBI>(s, l, uprev_ptr(s, l), u_ptr(s, l), (T)omega, 0, nullptr)));
+            if (!(it == 0 && skip_first))
+                CKS((launch_stencil<T, OP_JACOBI>(s, l, uprev_ptr(s, l), u_ptr(s, l), (T)omega, 0, nullptr)));
+            it++;
         }
     } else {
         for (int64_t it = 0; it < 2 * nsmooth; it++) {
@@ -704,7 +830,7 @@ int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns) {
 template <typename T>
 int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
     // Vcycle<T> (include/vcycle.h:14-98)
-    CKS(relax_t<T>(s, l, omega, ns));
+    CKS(relax_t<T>(s, l, omega, ns, /*later=*/l < s->levels - 1));
     if (l >= s->levels - 1) return MGP_OK;
     CKS(coarse_setup_t<T>(s, l, omega, ns));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
@@ -715,8 +841,8 @@ int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
 
 template <typename T>
 int fcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
-    // Fcycle<T> (include/fcycle.h:13-97)
-    CKS(relax_t<T>(s, l, omega, ns));
+    // Fcycle<T> (include/fcycle.h:13-97); the V-cycle of this level that follows relaxes it again
+    CKS(relax_t<T>(s, l, omega, ns, /*later=*/true));
     CKS(coarse_setup_t<T>(s, l, omega, ns));
     if (l < s->levels - 2) CKS(fcycle_t<T>(s, l + 1, omega, ns));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
@@ -1006,7 +1132,8 @@ void release(mgp_solver* s) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     s->graphs.clear();
     for (auto& L : s->lv) {
-        for (void* p : {L.ubuf[0], L.ubuf[1], L.f, L.r}) dev_free(s, p);
+        // with paired sweeps the three u buffers may sit in any of the slots
+        for (void* p : {L.ubuf[0], L.ubuf[1], L.spare, L.f, L.r}) dev_free(s, p);
         for (void* p : L.face) dev_free(s, p);
     }
     dev_free(s, s->d_norm);
@@ -1217,6 +1344,19 @@ static int create_plain(const mgp_desc* d, mgp_solver** out, const CreateCtx* ct
     for (int l = 0; l < s->levels; l++) {
         if (s->dtype == MGP_F64) tma_prepare_level<double>(s, s->lv[l]);
         else tma_prepare_level<float>(s, s->lv[l]);
+    }
+    {
+        int npair = 0;
+        for (int l = 0; l < s->levels; l++) {
+            cudaError_t e = s->dtype == MGP_F64 ? pair_prepare_level<double>(s, s->lv[l], npair)
+                                                : pair_prepare_level<float>(s, s->lv[l], npair);
+            if (e != cudaSuccess) {
+                release(s);
+                return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "sweep-pair buffer of level %d: %s",
+                            l, cudaGetErrorString(e));
+            }
+            npair += s->lv[l].pair;
+        }
     }
     cudaError_t e = dev_alloc(s, (void**)&s->d_norm, 64);
     if (e == cudaSuccess) e = dev_zero(s, s->d_norm, 64);

@@ -1518,6 +1518,9 @@ __global__ void __launch_bounds__(256) k_fill_uniform(double* f, Geom G, unsigne
 // halo entries of the staging copy are neither read (TO_DEV) nor written (!TO_DEV).
 template <typename T, bool TO_DEV>
 __global__ void __launch_bounds__(256) k_repack(T* dev, Geom G, T* stage, long long off, long long hs0, long long hs1) {
+    // launched as a programmatic dependent: wait for the previous grid (which may still be
+    // writing the field being downloaded, or reading the one being uploaded)
+    pdl_begin();
     const long long n = (long long)G.nx * G.ny * G.nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % G.nz);

@@ -40,6 +40,7 @@ FLAG_FUSED_SETUP = 8
 FLAG_REFINE_F32 = 16
 FLAG_REFINE_F64 = 32
 FLAG_TMA_SWEEPS = 64
+FLAG_SWEEP_PAIRS = 128
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,

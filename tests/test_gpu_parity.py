@@ -228,10 +228,10 @@ def test_strict_bc_cycle_bit_exact(mgp_mod, gpu_ready, ci):
         assert_field_equal(o, e, "u", l)
 
 
-def run_engine_solve(mgp, cfg, o_init):
+def run_engine_solve(mgp, cfg, o_init, flags=0):
     """Solve with the engine from the oracle's initial state (problem data computed on the
     host by the oracle, as PoissonSolver::init does)."""
-    e = make_engine(mgp, cfg, maxiter=cfg["maxiter"], tol=cfg["tol"])
+    e = make_engine(mgp, cfg, maxiter=cfg["maxiter"], tol=cfg["tol"], flags=flags)
     for name in ("u", "uprev", "f", "r"):
         if name == "uprev" and o_init.relaxation != 0:
             continue
