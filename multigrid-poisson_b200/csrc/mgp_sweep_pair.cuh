@@ -31,8 +31,9 @@
 //
 // Used only with MGP_FLAG_SWEEP_PAIRS.  Measured on B200 (513x257x129 FP64, bench workload):
 // 307-330 us per pair against 2 x 85 us for two single sweeps; removing the spills (768-thread
-// tiles) or every global load inside the plane step moved it by less than 10%, so the cost
-// lies in the per-plane barrier of one 30-warp CTA per SM and the instruction count.
+// tiles) or every global load inside the plane step moved it by less than 10%.  The copies of
+// a plane are issued after the per-plane barrier and waited for two planes later; with ~66 KB
+// in flight per CTA and ~4 us per plane step the kernel is short of bytes in flight.
 #pragma once
 
 namespace mgp {
