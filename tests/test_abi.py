@@ -123,3 +123,14 @@ def test_create_without_device_reports_no_device_or_succeeds(mgp_mod):
     with pytest.raises(mgp_mod.MgpError) as ei:
         mgp_mod.Solver((9, 9, 9), 2, 0.125)
     assert ei.value.status == mgp_mod.ERR_NO_DEVICE
+
+
+def test_missing_engine_library_fails_loudly(mgp_mod, monkeypatch, tmp_path):
+    """No CPU fallback: without libmgp.so every entry point of the Python layer raises."""
+    monkeypatch.setattr(mgp_mod, "_lib", None)
+    monkeypatch.setattr(mgp_mod, "LIB_PATH", tmp_path / "libmgp.so")
+    monkeypatch.setattr(mgp_mod._build, "needs_build", lambda: False)
+    with pytest.raises(RuntimeError, match="library missing"):
+        mgp_mod.lib()
+    with pytest.raises(RuntimeError, match="library missing"):
+        mgp_mod.Solver((9, 9, 9), 2, 0.125)
