@@ -189,12 +189,12 @@ def aggregate(units_per_rank: float, world: int, seconds_max: float) -> float:
     return units_per_rank * world / seconds_max
 
 
-def build_solver(mgp, device: int, maxiter: int, pinned: bool):
+def build_solver(mgp, device: int, maxiter: int, pinned: bool, flags: int = 0):
     st = mgp.Settings(levels=LEVELS, dims=list(DIMS), maxiter=maxiter, miniter=maxiter, tolerance=0.0,
                       h=H, origin=[0.0, 0.0, 0.0], dev=device)
     bc = mgp.BoundaryCondition(*BC)
     ps = mgp.PoissonSolver(st, bc, restriction="FullWeighting", relaxation="Jacobi", dtype=mgp.F64,
-                           pinned=pinned)
+                           pinned=pinned, flags=flags)
     ps.init(problem2, rhs2, dudx2, dudy2, dudz2)
     return ps
 
@@ -226,7 +226,7 @@ def run_kernels(args):
 
     import mgp
 
-    ps = build_solver(mgp, 0, maxiter=1, pinned=False)
+    ps = build_solver(mgp, 0, maxiter=1, pinned=False, flags=args.engine_flags)
     ps.to_device()
     eng = ps.engine
     stream = torch.cuda.ExternalStream(eng.stream_handle, device="cuda:0")
@@ -468,6 +468,31 @@ def cpu_reference(steps: int, warm: int, threads: int | None = None):
     return {"value": NDOF * iters / secs, "seconds": secs, "cycles": iters, "threads": threads}
 
 
+def cpu_reference_best(cycles: int, warm: int):
+    """The reference's CPU build at its fastest OpenMP thread count: one timed cycle at each of
+    1, 2, 4, ..., nproc threads (its build can be slower with more threads), then the bounded
+    sample of `cycles` cycles after `warm` warm-up cycles at the fastest count."""
+    nproc = os.cpu_count() or 1
+    counts = []
+    t = 1
+    while t < nproc:
+        counts.append(t)
+        t *= 2
+    counts.append(nproc)
+    sweep = {}
+    for t in counts:
+        r = cpu_reference(1, 0, threads=t)
+        if r is None:
+            return None
+        sweep[t] = r["value"]
+    best_t = max(sweep, key=sweep.get)
+    res = cpu_reference(cycles, warm, threads=best_t)
+    sweep[best_t] = max(sweep[best_t], res["value"])
+    res["sweep"] = {str(k): v for k, v in sorted(sweep.items())}
+    res["warm"] = warm
+    return res
+
+
 def run_reference_arm(args):
     world, rank, local, pg = dist_setup(args.gpus)
     if rank != 0:
@@ -477,36 +502,20 @@ def run_reference_arm(args):
     if not REF_BIN.exists():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref/ref_oracle not built"}))
         return 0
-    # Bounded sample: the reference takes ~1 s per F-cycle of this grid on 16 host threads, so
-    # at most REF_ARM_CYCLES timed cycles (after at most 2 warm-up cycles) keep the run to a
-    # minute or so whatever --steps says; the metric is per cycle, so the sample size does not
-    # change it.
-    nproc = os.cpu_count() or 1
-    # Thread sweep 1, 2, 4, ..., nproc: one timed cycle each below nproc (the reference's
-    # OpenMP build can be slower with more threads), the full sample at nproc; the line's
-    # value is the fastest.
-    sweep = {}
-    t = 1
-    while t < nproc:
-        r = cpu_reference(1, 0, threads=t)
-        sweep[t] = r["value"]
-        t *= 2
-    res = cpu_reference(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2), threads=nproc)
-    sweep[nproc] = res["value"]
-    best_t = max(sweep, key=sweep.get)
-    if best_t != nproc:
-        res = cpu_reference(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2), threads=best_t)
-        sweep[best_t] = max(sweep[best_t], res["value"])
+    # Bounded sample: the reference takes ~0.3-1 s per F-cycle of this grid, so at most
+    # REF_ARM_CYCLES timed cycles (after at most 2 warm-up cycles) keep the run to a minute or
+    # so whatever --steps says; the metric is per cycle, so the sample size does not change it.
+    res = cpu_reference_best(min(args.steps, REF_ARM_CYCLES), min(args.warmup, 2))
     cores = res["threads"]
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(1, res["cycles"]),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (analytic x^3 y^2 z problem)", "config": {"workload": WORKLOAD},
             "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"{int(res['cycles'])} F-cycles on the full grid after {args.warmup} "
-                                       f"warm-up cycles, OMP_NUM_THREADS={cores}"},
+                             "sample": f"{int(res['cycles'])} F-cycles on the full grid after {res['warm']} "
+                                       f"warm-up cycles, OMP_NUM_THREADS={cores} (fastest of a thread sweep)"},
             "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "thread_sweep": {str(k): v for k, v in sorted(sweep.items())}}
+            "thread_sweep": res["sweep"]}
     print(json.dumps(line))
     return 0
 
@@ -522,6 +531,8 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the mixed-precision, batched and served workloads")
     ap.add_argument("--served-requests", type=int, default=120)
+    ap.add_argument("--engine-flags", type=int, default=0,
+                    help="extra MGP_FLAG_* bits for the benchmarked solver (e.g. 64: TMA-fed sweeps)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -535,7 +546,7 @@ def main():
 
     torch.cuda.set_device(local)
     # Each rank: an independent replica of the whole solve on its own GPU.
-    ps = build_solver(mgp, local, maxiter=args.steps, pinned=True)
+    ps = build_solver(mgp, local, maxiter=args.steps, pinned=True, flags=args.engine_flags)
     ps.to_device()
     eng = ps.engine
     stream = torch.cuda.ExternalStream(eng.stream_handle, device=f"cuda:{local}")
@@ -599,7 +610,7 @@ def main():
     cpu = None
     if not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference(steps=CPU_BASELINE_CYCLES, warm=0)
+            cpu = cpu_reference_best(CPU_BASELINE_CYCLES, 0)
         except Exception as exc:  # noqa: BLE001 -- the baseline is informative only
             cpu = {"error": str(exc)}
     clocks = clk.summary()
@@ -632,7 +643,8 @@ def main():
     if cpu and "value" in cpu:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["threads"], "kind": "reference",
                                 "sample": f"{int(cpu['cycles'])} F-cycles of the same workload, reference OpenMP "
-                                          f"build, OMP_NUM_THREADS={cpu['threads']}"}
+                                          f"build, OMP_NUM_THREADS={cpu['threads']} (fastest of a thread sweep)",
+                                "thread_sweep": cpu.get("sweep")}
     elif cpu:
         line["cpu_baseline"] = {"error": cpu.get("error")}
     print(json.dumps(line))

@@ -311,9 +311,9 @@ int mgp_batch_restart(mgp_batch* b, int id);
  * shape[0] x shape[1] x shape[2] points of type dtype (MGP_F64 double, MGP_F32 float), point
  * (i,j,k) at a[i*stride[0] + j*stride[1] + k] (strides in elements), computed on `device`
  * on `stream` (a cudaStream_t, NULL = default stream); waits for the stream and writes the
- * norm to *out.  No counterpart in the reference: it is a variant of mgp_norm
- * (DeviceArray<T>::infinity_norm, include/devicearray.h:198-240) for callers that must not
- * allocate device memory.  It allocates nothing: its scratch is a static 256 KB device array.
+ * norm to *out.  No counterpart in the reference: it is a variant of mgp_norm for callers
+ * that must not allocate device memory.  It allocates nothing: its scratch is a static 256 KB
+ * device array.  A non-NULL stream must belong to `device`.
  *  - At most 268435456 (2^28) points; larger shapes return MGP_ERR_INVALID_ARG.
  *  - The first call on a device looks up the scratch array's address
  *    (cudaGetSymbolAddress); make that first call (an empty shape does only this setup)

@@ -119,10 +119,27 @@ int mgp_norm_device(int device, const void* a, int dtype, const int64_t shape[3]
                     n, kNsMaxPoints, kNsMaxBlocks, kNsChunk);
     if (n > 0) {
         if (!a) return fail(MGP_ERR_INVALID_ARG, "mgp_norm_device: null array");
-        if (stride[1] < shape[2] || stride[0] < stride[1] * shape[1])
-            return fail(MGP_ERR_INVALID_ARG, "mgp_norm_device: strides {%lld, %lld} overlap rows of shape {%lld, %lld, %lld}",
+        // rows must not overlap (stride[1] >= nz, stride[0] >= stride[1]*ny) and the last point's
+        // offset must fit in 64 bits; products are checked for overflow before they are compared
+        long long row = 0, last0 = 0, last1 = 0, last = 0;
+        const bool ovf = __builtin_mul_overflow((long long)stride[1], (long long)shape[1], &row) ||
+                         __builtin_mul_overflow((long long)stride[0], (long long)(shape[0] - 1), &last0) ||
+                         __builtin_mul_overflow((long long)stride[1], (long long)(shape[1] - 1), &last1) ||
+                         __builtin_add_overflow(last0, last1, &last) ||
+                         __builtin_add_overflow(last, (long long)shape[2], &last);
+        if (ovf || stride[1] < shape[2] || stride[0] < row)
+            return fail(MGP_ERR_INVALID_ARG, "mgp_norm_device: strides {%lld, %lld} overlap rows of shape {%lld, %lld, %lld}"
+                        " or overflow 64-bit offsets",
                         (long long)stride[0], (long long)stride[1], (long long)shape[0], (long long)shape[1],
                         (long long)shape[2]);
+    }
+    if (stream) {
+        int sdev = -1;
+        const cudaError_t e = cudaStreamGetDevice((cudaStream_t)stream, &sdev);
+        if (e != cudaSuccess)
+            return fail(MGP_ERR_INVALID_ARG, "mgp_norm_device: stream: %s", cudaGetErrorString(e));
+        if (sdev != device)
+            return fail(MGP_ERR_INVALID_ARG, "mgp_norm_device: the stream belongs to device %d, not %d", sdev, device);
     }
     DeviceGuard guard(device);
     NormScratch* scratch = nullptr;

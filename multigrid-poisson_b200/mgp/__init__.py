@@ -584,14 +584,14 @@ class PoissonSolver:
 
     def __init__(self, settings: Settings, bc: BoundaryCondition | None = None, restriction="Injection",
                  prolongation="TrilinearInterpolation", relaxation="GaussSeidel", dtype=F64, strict_bc=False,
-                 pinned=False):
+                 pinned=False, flags=0):
         if prolongation not in ("TrilinearInterpolation", TRILINEAR):
             raise ValueError(f"unknown prolongation {prolongation}")
         self.settings = settings
         self.BC = bc if bc is not None else BoundaryCondition()
         self.engine = Solver(settings.dims, settings.levels, settings.h, self.BC.as_list(), restriction, relaxation,
                              dtype, settings.maxiter, settings.miniter, settings.tolerance, settings.origin,
-                             settings.dev, strict_bc)
+                             settings.dev, strict_bc, flags=flags)
         lv0 = self.engine.level[0]
         dt = self.engine.np_dtype
         self._fields = {n: HostArray(lv0, dt, pinned) for n in FIELDS}

@@ -1,11 +1,15 @@
 #!/usr/bin/env bash
 # Builds the reference's own CPU path into oracle/_ref/ref_oracle (test infrastructure only).
 # Compiles oracle/ref_harness.cpp against the reference's unmodified include/ and src/ where
-# they lie (REF_DIR, default /root/reference); nothing from the reference is copied into the
-# repository.  Flags follow the reference's g++ configuration (config/g++.mkf) minus
+# they lie: the reference's source directory is the first argument (or REF_DIR); nothing from
+# the reference is copied into the repository.  Flags follow the reference's g++ configuration (config/g++.mkf) minus
 # -ffast-math, so the CPU arithmetic is plain IEEE double with no contraction.
 set -euo pipefail
-REF_DIR="${REF_DIR:-/root/reference}"
+REF_DIR="${1:-${REF_DIR:-}}"
+if [ -z "$REF_DIR" ]; then
+    echo "usage: build_ref.sh <reference source dir> (or set REF_DIR)" >&2
+    exit 2
+fi
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -d "$REF_DIR/include" ]; then

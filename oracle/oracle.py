@@ -46,14 +46,17 @@ def build_oracle(force: bool = False) -> Path:
     return LIB_PATH
 
 
-def build_ref() -> Path | None:
-    """Compile the reference's own CPU path (only where its sources are present)."""
-    ref_dir = os.environ.get("REF_DIR", "/root/reference")
-    if not Path(ref_dir, "include", "libpoisson.h").exists():
+def build_ref(ref_dir: str | None = None) -> Path | None:
+    """Compile the reference's own CPU path where its sources are present: `ref_dir`, else the
+    REF_DIR environment variable, else the installed copy under baseline/_ref.  Without any of
+    them the binary built earlier (if any) is returned."""
+    candidates = [ref_dir, os.environ.get("REF_DIR"), str(HERE.parent / "baseline" / "_ref")]
+    found = next((c for c in candidates if c and Path(c, "include", "libpoisson.h").exists()), None)
+    if found is None:
         return REF_BIN if REF_BIN.exists() else None
     src = HERE / "ref_harness.cpp"
     if not REF_BIN.exists() or REF_BIN.stat().st_mtime < src.stat().st_mtime:
-        subprocess.check_call(["bash", str(HERE / "build_ref.sh")])
+        subprocess.check_call(["bash", str(HERE / "build_ref.sh"), found])
     return REF_BIN
 
 

@@ -2,7 +2,7 @@
 
 Run where the reference sources are present (they are compiled by oracle/build_ref.sh):
 
-    python tests/golden/make_golden.py
+    REF_DIR=<reference source dir> python tests/golden/make_golden.py
 
 Writes ``tests/golden/solves.json`` (whole PoissonSolver::solve runs: final relative
 residual, reported iterations, and SHA-256 digests of the level-0 solution and residual

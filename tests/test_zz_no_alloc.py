@@ -111,3 +111,51 @@ def test_empty_shape_and_limit(mgp_mod, gpu_ready):
     rc, _ = _norm_device(mgp_mod, t, dt, shape=(LIMIT // (4 * 4) + 1, 4, 4))
     assert rc == mgp_mod.ERR_INVALID_ARG
     assert b"static scratch limit" in mgp_mod.lib().mgp_last_error()
+
+
+def test_calls_leave_free_device_memory_unchanged(mgp_mod, gpu_ready):
+    """The property the entry point exists for: after its one-time set-up (an empty-shape
+    call), many calls on a large array and a small one take no device memory."""
+    import torch
+
+    dt = mgp_mod.F64
+    e_big, big = _engine_and_values(mgp_mod, (257, 129, 65), dt, seed=8, scale=2.0)
+    e_small, small = _engine_and_values(mgp_mod, (17, 9, 33), dt, seed=9)
+    tb, ts = _device_copy(big, pad_z=3), _device_copy(small, pad_z=7)
+    rc, _ = _norm_device(mgp_mod, tb, dt, shape=(0, 1, 1))
+    assert rc == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    want_big, want_small = e_big.norm("f", 0), e_small.norm("f", 0)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    for _ in range(50):
+        rc, v = _norm_device(mgp_mod, tb, dt)
+        assert rc == 0 and v == want_big
+    rc, v = _norm_device(mgp_mod, ts, dt)
+    assert rc == 0 and v == want_small
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info(0)
+    assert free2 == free1, f"free device memory changed by {free1 - free2} bytes over the calls"
+    assert free1 == free0
+    e_big.close()
+    e_small.close()
+
+
+def test_rejects_a_stream_of_another_device_and_overflowing_strides(mgp_mod, gpu_ready):
+    import torch
+
+    dt = mgp_mod.F64
+    t = torch.zeros((4, 4, 4), dtype=torch.float64, device="cuda:0")
+    f = _bind(mgp_mod)
+    out = ctypes.c_double(-1.0)
+    shp = (ctypes.c_int64 * 3)(4, 4, 4)
+    huge = (ctypes.c_int64 * 2)(1 << 62, 1 << 61)  # stride[1] * ny overflows 64 bits
+    rc = f(0, t.data_ptr(), dt, shp, huge, None, ctypes.byref(out))
+    assert rc == mgp_mod.ERR_INVALID_ARG
+    assert b"overflow" in mgp_mod.lib().mgp_last_error()
+    if torch.cuda.device_count() > 1:
+        s1 = torch.cuda.Stream(device="cuda:1")
+        ok = (ctypes.c_int64 * 2)(16, 4)
+        rc = f(0, t.data_ptr(), dt, shp, ok, s1.cuda_stream, ctypes.byref(out))
+        assert rc == mgp_mod.ERR_INVALID_ARG
