@@ -234,6 +234,10 @@ def run_kernels(args):
     nc = ((DIMS[0] >> 1) + 1) * ((DIMS[1] >> 1) + 1) * ((DIMS[2] >> 1) + 1)
     ops = {  # name: (callable, algorithmic bytes per launch)
         "jacobi_sweep": (lambda: eng.relax(0, -1.0, 1), 24.0 * n),
+        # two sweeps in one pass: read u, f; write u2 and u1
+        "jacobi_pair": (lambda: eng.relax(0, -1.0, 2), 32.0 * n),
+        # two sweeps and the residual with its max-norm in one pass: read u, f; write u2, u1, r
+        "pair_residual_norm": (lambda: eng.relax_residual(0, -1.0, 2, norm=True), 40.0 * n),
         "residual": (lambda: eng.residual(0), 24.0 * n),
         "restrict_fw": (lambda: eng.restrict(0), 8.0 * (n + nc)),
         "prolong_add": (lambda: eng.prolong_add(0), 8.0 * (2 * n + nc)),

@@ -71,13 +71,12 @@ typedef enum { MGP_CYCLE_RELAXATION = 0, MGP_CYCLE_V = 1, MGP_CYCLE_F = 2 } mgp_
                                  reference's resolution to Dirichlet (include/domain.h:140-145,191-192) */
 #define MGP_FLAG_REFINE_F32 16u /* iterative refinement, FP32 correction hierarchy (see mgp_solve) */
 #define MGP_FLAG_REFINE_F64 32u /* iterative refinement, FP64 correction hierarchy */
-#define MGP_FLAG_TMA_SWEEPS 64u /* levels of >= 2^20 points sweep with the TMA-fed kernel (shared-memory plane
-                                  rings filled by cp.async.bulk.tensor) instead of the per-thread cp.async march */
-#define MGP_FLAG_SWEEP_PAIRS 128u /* Jacobi relaxations of levels of >= 2^20 points make
-                                    consecutive sweeps two at a time in one pass (k_jacobi_pair:
-                                    same results, one more level-sized buffer per such level).  Off
-                                    by default: on B200 the pair still takes longer than two
-                                    single sweeps (513x257x129 FP64: 307-330 us against 2 x 85 us) */
+#define MGP_FLAG_WAVE 256u /* Jacobi levels of >= 2^20 points relax with the TMA-fed wavefront pass: two
+                             sweeps, and the residual that follows them, in one march over HBM (same
+                             results; one more level-sized buffer per such level).  Off by default: on
+                             B200 the pass is bound by instruction issue, not HBM, and takes longer
+                             than the separate passes (513x257x129 FP64: two sweeps 234 us against
+                             2 x 85 us) */
 #define MGP_FLAG_FUSED_SETUP 8u /* cycles form the residual inside the restriction kernel (one
                                    launch, r never stored) on every level; without the flag only
                                    levels of at most 2^20 points do */
@@ -200,6 +199,18 @@ int mgp_set_iteration_limits(mgp_solver* s, int64_t maxiter, int64_t miniter, do
  * half-sweeps (Jacobi ping-pong / red-black SOR) with the Neumann ghost values formed in
  * the kernel. */
 int mgp_relax(mgp_solver* s, int level, double omega, int64_t nsmooth);
+/* Failure detection of the wavefront passes (MGP_FLAG_WAVE): bound on the polls of a wait for a
+ * plane copy (0 = the default, 2^22).  A wait that runs out marks the pass failed; the pass
+ * still lets every copy it issued land before it exits, and the next norm read-back (the solve
+ * loop's) returns MGP_ERR_TIMEOUT.  No counterpart in the reference (its target regions are
+ * synchronous); a test sets a bound of 1 to drive the failure path without a GPU fault. */
+int mgp_set_wait_polls(mgp_solver* s, int64_t polls);
+/* Relaxation<T>::relax followed by residual<T> (include/relaxation.h:19-94,
+ * include/residual.h:17-81) and, when norm != NULL, the max-norm of r over the shape
+ * (DeviceArray<T>::infinity_norm, include/devicearray.h:198-240): the solve loop's step on a
+ * single level (include/libpoisson.h:294-330).  Same results as mgp_relax, mgp_residual and
+ * mgp_norm in turn; on large Jacobi levels the last sweeps and the residual share one pass. */
+int mgp_relax_residual(mgp_solver* s, int level, double omega, int64_t nsmooth, double* norm);
 /* residual<T>(Domain&) (include/residual.h:17-81). */
 int mgp_residual(mgp_solver* s, int level);
 /* Restriction<T>::restrict_to(r_l, f_{l+1}) (injection.h:29-67 / fullweighting.h:37-122). */

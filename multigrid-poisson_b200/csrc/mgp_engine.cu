@@ -28,8 +28,7 @@
 
 #include "mgp.h"
 #include "mgp_kernels.cuh"
-#include "mgp_stencil_tma.cuh"
-#include "mgp_sweep_pair.cuh"
+#include "mgp_wave.cuh"
 
 using namespace mgp;
 
@@ -89,19 +88,20 @@ struct LevelState {
     bool first_done = false;  // the set-up of the finer level already did this level's first sweep
     bool gs_column = false; // padded y extent even: colour depends on (j,k) only; whole columns
     mgp_level_info info;    // host (reference) layout
-    // TMA-fed stencil sweeps (large levels): tensor maps of both u buffers and of f
-    bool tma = false;
-    CUtensorMap map_u[2];
-    CUtensorMap map_f;
-    TmaTiling tiling;
-    // Paired Jacobi sweeps (large levels, k_jacobi_pair): a third level-sized buffer rotates
-    // with the two of the ping-pong pair; phys[] are the three allocations in their original
-    // order, whose arrangement over (ubuf[0], ubuf[1], spare) is part of the graph state.
+    // Wavefront passes (k_wave, large Jacobi levels): sweeps two at a time and the residual of
+    // the last sweep in the same pass.  Two sweeps in one pass write u2 into a third level-sized
+    // buffer that rotates with the two of the ping-pong pair; phys[] are the three allocations
+    // in their original order, whose arrangement over (ubuf[0], ubuf[1], spare) is part of the
+    // graph state.  wt[M] / wmap_*[M]: tiling and tensor maps of the M-stage passes.
     bool pair = false;
     void* spare = nullptr;
     void* phys[3] = {nullptr, nullptr, nullptr};
-    int pair_tj = 0, pair_nvec = 0, pair_grid = 0;
-    size_t pair_smem = 0;
+    bool wave = false;
+    WaveTile wt[4];
+    CUtensorMap wmap_u[4][3];   // u0 planes, per allocation
+    CUtensorMap wmap_f[4];
+    CUtensorMap wmap_bk[4][3];  // u_prev's k = 0 / nz-1 columns (V x rows boxes), per allocation
+    CUtensorMap wmap_bj[3];     // u_prev's j = 0 / ny-1 rows (P x 1 boxes), per allocation
 };
 
 struct GraphEntry {
@@ -138,6 +138,7 @@ struct mgp_solver {
     // batch's pinned slab.
     cudaMemPool_t pool = nullptr;
     bool owns_h_norm = true;
+    unsigned wait_polls = kWaitPolls;  // bound of the wavefront passes' waits for a copy
 };
 
 // Where a solver's memory comes from: nullptr = its own stream, cudaMalloc, pinned read-back.
@@ -318,12 +319,7 @@ void hsq_terms(T hsq, T& inv, int& pow2) {
     if (pow2 && !std::isnormal((double)inv)) pow2 = 0;
 }
 
-// ---- TMA-fed sweeps ------------------------------------------------------------------------
-// With MGP_FLAG_TMA_SWEEPS, levels of at least kTmaMinPoints points (and at least 3 points per
-// axis) sweep with k_stencil_tma.  Off by default: on B200 the per-thread cp.async march of
-// k_stencil is faster (513x257x129 FP64 Jacobi sweep 85 us against 128-140 us).
-constexpr long long kTmaMinPoints = 1ll << 20;
-
+// ---- tensor maps ----------------------------------------------------------------------------
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -355,124 +351,228 @@ bool encode_field_map(CUtensorMap* m, void* base, bool f64, const Geom& G, int b
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Tiles of kTmaTJ rows x BK points: BK is the largest multiple of V and HK that keeps a u box
-// within 256 elements and a CTA within kTmaMaxThreads threads, evened out over the k tiles.
-template <typename T>
-TmaTiling tma_tiling(const Geom& G) {
-    constexpr int V = VecT<T>::V, HK = tma_hk<T>(), Q = V > HK ? V : HK;
-    int bkmax = std::min(256 - 2 * HK, (kTmaMaxThreads / kTmaTJ) * V) / Q * Q;
-    TmaTiling t;
-    t.ntk = (G.nz + bkmax - 1) / bkmax;
-    t.BK = ((G.nz + t.ntk - 1) / t.ntk + Q - 1) / Q * Q;
-    t.ntj = (G.ny + kTmaTJ - 1) / kTmaTJ;
-    t.nvec = t.BK / V;
-    t.slot_u = (int)(((size_t)(kTmaTJ + 2) * (t.BK + 2 * HK) * sizeof(T) + 127) / 128 * 128);
-    t.slot_f = (int)(((size_t)kTmaTJ * t.BK * sizeof(T) + 127) / 128 * 128);
-    t.work = (long long)t.ntj * t.ntk * G.nx;
-    t.whole_tiles = 0;
-    return t;
+// ---- wavefront passes ---------------------------------------------------------------------
+// Jacobi levels of at least kWaveMinPoints points (at least 3 per axis, nz small enough for one
+// TMA box row) relax with k_wave: two sweeps per pass, and the residual that follows the last
+// sweep (the coarse-grid set-up's, or the solve loop's with its max-norm) in the same pass,
+// with MGP_FLAG_WAVE (opt-in: on B200 the pass is issue-bound and slower than the separate
+// passes).  Solvers carved from a batch pool
+// sweep with the batch engine's own kernels.
+constexpr long long kWaveMinPoints = 1ll << 20;
+constexpr size_t kWaveMaxSmem = 224 * 1024;  // dynamic; the static barriers and reduction slots fit beside it
+
+// Tiling of an M-stage pass: TJ output rows per CTA (thread rows TJ + 2(M-1), one 16-byte
+// k-vector each, at most kWaveMaxThreads threads and kWaveMaxSmem bytes of rings), and the
+// chunk count along i.  Among those, the one with the least work per SM: CTAs per SM x steps
+// per chunk (its planes plus the 2(M-1) a chunk re-computes at its ends) x thread rows (the
+// TJ rows of the tile plus the halo rows it re-computes), plus one for the copied halo rows.  The CTAs of one chunk run together,
+// so halo rows come from L2.
+// Pipeline depths of the wavefront passes: u0 ring slots, f planes in flight, L2 prefetch
+// distance and kind.  MGP_WAVE_RU / _FA / _L2A / _L2MODE override them (experiments).
+struct WaveDepth {
+    int ru = 6, fa = 3, l2a = 6, l2mode = 2;
+};
+WaveDepth wave_depth() {
+    static const WaveDepth d = [] {
+        WaveDepth w;
+        auto env = [](const char* n, int& v, int lo, int hi) {
+            const char* e = std::getenv(n);
+            if (e && *e) v = std::max(lo, std::min(hi, std::atoi(e)));
+        };
+        env("MGP_WAVE_RU", w.ru, 3, kWaveMaxRing);
+        env("MGP_WAVE_FA", w.fa, 1, kWaveMaxRing - 1);
+        env("MGP_WAVE_L2A", w.l2a, 0, 32);
+        env("MGP_WAVE_L2MODE", w.l2mode, 0, 2);
+        return w;
+    }();
+    return d;
 }
 
 template <typename T>
-size_t tma_smem(const TmaTiling& t) {
-    return (size_t)kTmaRingU * t.slot_u + (size_t)kTmaRingF * t.slot_f + 128;
-}
-
-template <typename T>
-void tma_prepare_level(mgp_solver* s, LevelState& L) {
-    L.tma = false;
-    const Geom& G = L.G;
-    if (!(s->desc.flags & MGP_FLAG_TMA_SWEEPS) || (long long)G.nx * G.ny * G.nz < kTmaMinPoints || G.nx < 3 ||
-        G.ny < 3 || G.nz < 3)
-        return;
-    constexpr int HK = tma_hk<T>();
-    L.tiling = tma_tiling<T>(G);
-    const bool f64 = sizeof(T) == 8;
-    const int bu = L.tiling.BK + 2 * HK, bf = L.tiling.BK;
-    bool ok = encode_field_map(&L.map_u[0], L.ubuf[0], f64, G, bu, kTmaTJ + 2) &&
-              encode_field_map(&L.map_f, L.f, f64, G, bf, kTmaTJ);
-    if (ok && L.ubuf[1]) ok = encode_field_map(&L.map_u[1], L.ubuf[1], f64, G, bu, kTmaTJ + 2);
-    else L.map_u[1] = L.map_u[0];
-    L.tma = ok;
-}
-
-// Launch of k_stencil_tma; src must be one of the level's u buffers.
-template <typename T, int OP, bool NORM>
-int launch_stencil_tma(mgp_solver* s, int l, const StencilArgs<T>& a) {
-    LevelState& L = s->lv[l];
-    const CUtensorMap& mu = a.src == L.ubuf[0] ? L.map_u[0] : L.map_u[1];
-    TmaTiling t = L.tiling;
-    const size_t smem = tma_smem<T>(t);
-    auto kernel = k_stencil_tma<T, OP, NORM>;
-    static bool attr_set[64] = {};  // per instantiation and device
-    if (s->device < 64 && !attr_set[s->device]) {
-        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set[s->device] = true;
-    }
-    const int threads = kTmaTJ * t.nvec;
-    int grid;
-    if (OP == OP_GS_COLUMN) {
-        t.whole_tiles = 1;
-        grid = t.ntj * t.ntk;
-    } else {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-            per_sm = 1;
-        grid = (int)std::min<long long>(t.work, (long long)sm_count(s->device) * per_sm);
-    }
-    return launch_k_ordered(s, kernel, dim3(grid), dim3(threads), smem, mu, L.map_f, a, t, s->err_word);
-}
-
-// ---- paired Jacobi sweeps ----------------------------------------------------------------
-// With MGP_FLAG_SWEEP_PAIRS, levels of at least kPairMinPoints points (at least 3 per axis) make
-// consecutive Jacobi sweeps two at a time with k_jacobi_pair, unless the level sweeps with the
-// TMA-fed kernel or the solver is carved from a batch pool (the batch engine sweeps with its own
-// kernels).  Off by default: on B200 one pair launch of the 513x257x129 FP64 level takes
-// 307-330 us, two single sweeps 2 x 85 us.  A CTA covers tj+2 rows of nvec vectors (at most 1024 threads, tj >= 4);
-// tj is the largest that fits, evened out over the tiles of a plane.
-constexpr long long kPairMinPoints = 1ll << 20;
-constexpr size_t kPairMaxSmem = 200 * 1024;
-
-template <typename T>
-cudaError_t pair_prepare_level(mgp_solver* s, LevelState& L, int npair) {
+WaveTile wave_tiling(const Geom& G, int M, int sms, const WaveDepth& d) {
     constexpr int V = VecT<T>::V;
+    constexpr long long ES = sizeof(T);
+    WaveTile best;
+    const int nvec = (G.nz + V - 1) / V;
+    const int P = nvec * V;
+    if (P > kWaveMaxWidth || nvec < 3) return best;  // a row needs interior vectors besides its two ends
+    auto rup = [](long long n) { return (int)((n + 127) / 128 * 128); };
+    double best_cost = 1e300;
+    int tj_only = 0;  // MGP_WAVE_TJ<M>: an experiment's fixed tile height
+    {
+        char name[16];
+        std::snprintf(name, sizeof(name), "MGP_WAVE_TJ%d", M);
+        if (const char* e = std::getenv(name); e && *e) tj_only = std::atoi(e);
+    }
+    for (int TJ = 1; TJ <= G.ny; TJ++) {
+        if (tj_only > 0 && TJ != tj_only) continue;
+        const int rows = TJ + 2 * (M - 1);
+        if (rows * nvec > kWaveMaxThreads || rows + 2 > 256) break;
+        // a u0 slot: the (rows+2) x P box, then u_prev's k = 0 and k = nz-1 columns (rows x V
+        // each) and its j = 0 and j = ny-1 rows (P each)
+        const int bk = rup(rows * V * ES), bj = rup(P * ES);
+        const int u_box = rup((long long)(rows + 2) * P * ES);
+        const int su = u_box + 2 * bk + 2 * bj, sf = rup((long long)rows * P * ES), sw = sf;
+        const size_t smem = 256 + (size_t)d.ru * su + (size_t)(M + d.fa) * sf + (size_t)2 * (M - 1) * sw;
+        if (smem > kWaveMaxSmem) break;
+        const int tiles_j = (G.ny + TJ - 1) / TJ;
+        for (int c = 1; c <= G.nx; c++) {
+            const int ci = (G.nx + c - 1) / c;
+            if ((G.nx + ci - 1) / ci != c) continue;
+            const long long per_sm = ((long long)tiles_j * c + sms - 1) / sms;
+            if (per_sm > 16) break;
+            // steps of a chunk: its planes, the 2(M-1) it re-computes at its ends, and about
+            // three for the copies that fill the rings before the first step
+            const double cost = (double)per_sm * (ci + 2 * (M - 1) + 3) * (rows + 1);
+            if (cost < best_cost * (1.0 - 1e-9)) {
+                best_cost = cost;
+                best.ok = true;
+                best.TJ = TJ;
+                best.rows = rows;
+                best.nvec = nvec;
+                best.P = P;
+                best.tiles_j = tiles_j;
+                best.ci = ci;
+                best.chunks = c;
+                best.slot_u = su;
+                best.slot_f = sf;
+                best.slot_w = sw;
+                best.b_klo = u_box;
+                best.b_khi = u_box + bk;
+                best.b_jlo = u_box + 2 * bk;
+                best.b_jhi = u_box + 2 * bk + bj;
+                best.kl = (G.nz - 1) / V * V;
+                best.ru = d.ru;
+                best.fa = d.fa;
+                best.l2a = d.l2a;
+                best.l2mode = d.l2mode;
+                best.smem = smem;
+            }
+        }
+    }
+    return best;
+}
+
+// A 3-D map (k, j, i) of a pitched field with a (P, rows, 1) box; reads outside the level's
+// shape are zero-filled.
+bool encode_wave_map(CUtensorMap* m, void* base, bool f64, const Geom& G, int P, int rows) {
+    return encode_field_map(m, base, f64, G, P, rows);
+}
+
+template <typename T>
+cudaError_t wave_prepare_level(mgp_solver* s, LevelState& L, int npair) {
+    L.wave = false;
     L.pair = false;
     const Geom& G = L.G;
-    if (s->desc.relaxation != MGP_JACOBI || !(s->desc.flags & MGP_FLAG_SWEEP_PAIRS) || s->pool || L.tma ||
-        !L.ubuf[1] || s->levels > 31 || npair >= kPairMaxLevels || (long long)G.nx * G.ny * G.nz < kPairMinPoints ||
-        G.nx < 3 || G.ny < 3 || G.nz < 3)
+    if (s->desc.relaxation != MGP_JACOBI || !(s->desc.flags & MGP_FLAG_WAVE) || s->pool || !L.ubuf[1] ||
+        s->levels > 31 || npair >= kPairMaxLevels || (long long)G.nx * G.ny * G.nz < kWaveMinPoints || G.nx < 3 ||
+        G.ny < 3 || G.nz < 3 || !encode_tiled())
         return cudaSuccess;
-    const int nvec = (G.nz + V - 1) / V;
-    int tjmax = kPairMaxThreads / nvec - 2;
-    while (tjmax >= 4 && pair_smem_elems(tjmax, nvec, V) * sizeof(T) > kPairMaxSmem) tjmax--;
-    if (tjmax < 4) return cudaSuccess;
-    const int ntiles = (G.ny + tjmax - 1) / tjmax;
-    const int tj = (G.ny + ntiles - 1) / ntiles;
-    const size_t smem = pair_smem_elems(tj, nvec, V) * sizeof(T);
-    const int threads = (tj + 2) * nvec;
-    cudaError_t e = cudaFuncSetAttribute(k_jacobi_pair<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kPairMaxSmem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_jacobi_pair<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kPairMaxSmem);
-    int per_sm = 0;
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_pair<T, true>, threads, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaSuccess;
-    const long long work = (long long)ntiles * G.nx;
-    e = dev_alloc(s, &L.spare, L.elems * sizeof(T));
+    for (int M = 1; M <= 3; M++) {
+        L.wt[M] = wave_tiling<T>(G, M, sm_count(s->device), wave_depth());
+        if (!L.wt[M].ok) return cudaSuccess;
+    }
+    cudaError_t e = dev_alloc(s, &L.spare, L.elems * sizeof(T));
     if (e == cudaSuccess) e = dev_zero(s, L.spare, L.elems * sizeof(T));
     if (e != cudaSuccess) return e;
     L.phys[0] = L.ubuf[0];
     L.phys[1] = L.ubuf[1];
     L.phys[2] = L.spare;
-    L.pair_tj = tj;
-    L.pair_nvec = nvec;
-    L.pair_smem = smem;
-    L.pair_grid = (int)std::min<long long>(work, (long long)sm_count(s->device) * per_sm);
+    const bool f64 = sizeof(T) == 8;
+    bool ok = true;
+    constexpr int V = VecT<T>::V;
+    for (int M = 1; M <= 3 && ok; M++) {
+        const WaveTile& t = L.wt[M];
+        for (int b = 0; b < 3 && ok; b++) {
+            ok = encode_wave_map(&L.wmap_u[M][b], L.phys[b], f64, G, t.P, t.rows + 2) &&
+                 encode_wave_map(&L.wmap_bk[M][b], L.phys[b], f64, G, V, t.rows);
+        }
+        if (ok) ok = encode_wave_map(&L.wmap_f[M], L.f, f64, G, t.P, t.rows);
+    }
+    for (int b = 0; b < 3 && ok; b++) ok = encode_wave_map(&L.wmap_bj[b], L.phys[b], f64, G, L.wt[1].P, 1);
+    if (!ok) {
+        dev_free(s, L.spare);
+        L.spare = nullptr;
+        return cudaSuccess;
+    }
     L.pair = true;
+    L.wave = true;
+    if (const char* e = std::getenv("MGP_WAVE_VERBOSE"); e && *e == '1') {
+        for (int M = 1; M <= 3; M++) {
+            const WaveTile& t = L.wt[M];
+            std::fprintf(stderr, "wave %dx%dx%d M=%d: TJ=%d rows=%d threads=%d grid=%dx%d ci=%d smem=%zu ru=%d fa=%d l2a=%d l2mode=%d\n",
+                         G.nx, G.ny, G.nz, M, t.TJ, t.rows, t.rows * t.nvec, t.tiles_j, t.chunks, t.ci, t.smem, t.ru,
+                         t.fa, t.l2a, t.l2mode);
+        }
+    }
     return cudaSuccess;
+}
+
+template <typename T, int NJ, int RES, bool WU1>
+int launch_wave_k(mgp_solver* s, const WaveTile& t, const CUtensorMap& mu, const CUtensorMap& mf,
+                  const CUtensorMap& mbk, const CUtensorMap& mbj, const WaveArgs<T>& a) {
+    auto kernel = k_wave<T, NJ, RES, WU1>;
+    static bool attr_set[64] = {};  // per instantiation and device
+    if (s->device < 64 && !attr_set[s->device]) {
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveMaxSmem));
+        attr_set[s->device] = true;
+    }
+    // the consumer threads in whole warps, then the producer warp
+    const unsigned threads = (unsigned)((t.rows * t.nvec + 31) / 32 * 32 + 32);
+    return launch_k(s, kernel, dim3((unsigned)(t.tiles_j * t.chunks)), dim3(threads), t.smem, mu, mf, mbk, mbj, a);
+}
+
+// nj Jacobi sweeps (1 or 2) of level l in one pass, then (res != 0) the residual of their
+// result: r stored, and with res == 2 its max-norm into *norm.  Buffers as Relaxation::relax
+// leaves them: one sweep -> u_prev's buffer becomes u; two sweeps -> the spare buffer takes u2
+// and becomes u, u_prev takes u1 when wu1 (else its relaxed points are left stale), and the old
+// u becomes the spare.
+template <typename T>
+int launch_wave(mgp_solver* s, int l, int nj, int res, bool wu1, T omega, unsigned long long* norm) {
+    LevelState& L = s->lv[l];
+    const int M = nj + (res ? 1 : 0);
+    const WaveTile& t = L.wt[M];
+    WaveArgs<T> a;
+    a.G = L.G;
+    a.A = (const T*)u_ptr(s, l);
+    a.B = (T*)uprev_ptr(s, l);
+    a.C = (T*)L.spare;
+    a.r = (T*)L.r;
+    a.f = (const T*)L.f;
+    a.F = faces_of<T>(s, l);
+    // the constants of launch_stencil (jacobi.h:41-44, residual.h, neumann.h:117)
+    a.two_h = (T)(2.0 * L.h);
+    a.hsq = (T)(L.h * L.h);
+    a.one_omega = (T)(1.0 - omega);
+    a.omega_sixth = (T)(omega / 6.0);
+    hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
+    a.t = t;
+    a.norm = norm;
+    a.err = s->err_word;
+    a.wait_polls = s->wait_polls;
+    const int ia = phys_index(L, a.A), ib = phys_index(L, a.B);
+    const CUtensorMap& mu = L.wmap_u[M][ia];
+    const CUtensorMap& mf = L.wmap_f[M];
+    const CUtensorMap& mbk = L.wmap_bk[M][ib];
+    const CUtensorMap& mbj = L.wmap_bj[ib];
+    int st;
+#define MGP_WAVE(NJ_, RES_, WU1_) launch_wave_k<T, NJ_, RES_, WU1_>(s, t, mu, mf, mbk, mbj, a)
+    if (nj == 1) {
+        if (res == 0) st = MGP_WAVE(1, 0, false);
+        else if (res == 1) st = MGP_WAVE(1, 1, false);
+        else st = MGP_WAVE(1, 2, false);
+    } else if (res == 0) {
+        st = wu1 ? MGP_WAVE(2, 0, true) : MGP_WAVE(2, 0, false);
+    } else if (res == 1) {
+        st = wu1 ? MGP_WAVE(2, 1, true) : MGP_WAVE(2, 1, false);
+    } else {
+        st = wu1 ? MGP_WAVE(2, 2, true) : MGP_WAVE(2, 2, false);
+    }
+#undef MGP_WAVE
+    CKS(st);
+    if (nj == 1) L.cur ^= 1;
+    else std::swap(L.ubuf[L.cur], L.spare);
+    return MGP_OK;
 }
 
 // ---- stencil launches -------------------------------------------------------------------
@@ -494,10 +594,6 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     hsq_terms(a.hsq, a.inv_hsq, a.hsq_pow2);
     a.colour = colour;
     a.norm = norm;
-    if (L.tma && (src == L.ubuf[0] || src == L.ubuf[1])) {
-        if (OP == OP_RESIDUAL && norm) return launch_stencil_tma<T, OP, true>(s, l, a);
-        return launch_stencil_tma<T, OP, false>(s, l, a);
-    }
     constexpr int V = VecT<T>::V;
     const int plane = L.G.ny * ((L.G.nz + V - 1) / V);  // threads per plane
     const int bx = (plane + kThreads - 1) / kThreads;
@@ -515,55 +611,49 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     return launch_k(s, k_stencil<T, OP, false>, grid, dim3(kThreads), 0, a);
 }
 
-// Two Jacobi sweeps in one pass (k_jacobi_pair): u0 = u, u1 -> u_prev (write_u1), u2 -> the
-// spare buffer, which then becomes u; the old u becomes the spare.
-template <typename T>
-int launch_pair(mgp_solver* s, int l, T omega, bool write_u1) {
-    LevelState& L = s->lv[l];
-    PairArgs<T> a;
-    a.G = L.G;
-    a.src = (const T*)u_ptr(s, l);
-    a.prev = (T*)uprev_ptr(s, l);
-    a.out = (T*)L.spare;
-    a.f = (const T*)L.f;
-    a.F = faces_of<T>(s, l);
-    // the constants of launch_stencil (jacobi.h:41-44, neumann.h:117)
-    a.two_h = (T)(2.0 * L.h);
-    a.hsq = (T)(L.h * L.h);
-    a.one_omega = (T)(1.0 - omega);
-    a.omega_sixth = (T)(omega / 6.0);
-    a.tj = L.pair_tj;
-    a.nvec = L.pair_nvec;
-    a.work = (long long)((L.G.ny + L.pair_tj - 1) / L.pair_tj) * L.G.nx;
-    const dim3 block((unsigned)((L.pair_tj + 2) * L.pair_nvec));
-    if (write_u1) CKS(launch_k(s, k_jacobi_pair<T, true>, dim3(L.pair_grid), block, L.pair_smem, a));
-    else CKS(launch_k(s, k_jacobi_pair<T, false>, dim3(L.pair_grid), block, L.pair_smem, a));
-    std::swap(L.ubuf[L.cur], L.spare);
-    return MGP_OK;
-}
+// Residual requests a relaxation may take over: on wavefront levels the pass of its last
+// sweep also forms the residual of the result -- r stored (the coarse-grid set-up's residual),
+// or r stored with its max-norm (the solve loop's).
+enum { RESID_NONE = 0, RESID_STORE = 1, RESID_NORM = 2 };
 
 // later: another relaxation of this level follows in the same cycle before anything reads
 // u_prev (the pre-smoothing of a V- or F-cycle), so a sweep pair that ends the call may leave
 // u_prev's relaxed points stale: that later relaxation overwrites all of them.
+// resid / norm: a residual request (above); *resid_done tells whether it was taken over (the
+// caller forms the residual itself otherwise).
 template <typename T>
-int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth, bool later = false) {
+int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth, bool later = false, int resid = RESID_NONE,
+            unsigned long long* norm = nullptr, bool* resid_done = nullptr) {
     // Relaxation<T>::relax (include/relaxation.h:19-94)
     LevelState& L = s->lv[l];
+    if (resid_done) *resid_done = false;
     // first_done: the coarse-grid set-up that just zeroed this level also wrote its first sweep
     const bool skip_first = L.first_done;
     L.first_done = false;
     if (s->desc.relaxation == MGP_JACOBI) {
-        for (int64_t it = 0; it < nsmooth;) {
-            if (L.pair && nsmooth - it >= 2 && !(it == 0 && skip_first)) {
-                // two swap_u's leave the current-buffer index as it was
-                CKS(launch_pair<T>(s, l, (T)omega, it + 2 >= nsmooth && !later));
-                it += 2;
-                continue;
+        int64_t it = 0;
+        if (skip_first && nsmooth > 0) {
+            L.cur ^= 1;  // that sweep's swap_u
+            it = 1;
+        }
+        if (L.wave) {
+            // the fused residual multiplies by 1/h^2, which is exact where h^2 is a power of two
+            T hsq = (T)(L.h * L.h), inv;
+            int pow2 = 0;
+            hsq_terms(hsq, inv, pow2);
+            while (it < nsmooth) {
+                const int nj = nsmooth - it >= 2 ? 2 : 1;
+                const bool last = it + nj >= nsmooth;
+                const int res = last && pow2 ? resid : RESID_NONE;
+                CKS(launch_wave<T>(s, l, nj, res, nj == 2 && last && !later, (T)omega, norm));
+                if (res != RESID_NONE && resid_done) *resid_done = true;
+                it += nj;
             }
+            return MGP_OK;
+        }
+        for (; it < nsmooth; it++) {
             L.cur ^= 1;  // swap_u: the previous iterate becomes the source
-            if (!(it == 0 && skip_first))
-                CKS((launch_stencil<T, OP_JACOBI>(s, l, uprev_ptr(s, l), u_ptr(s, l), (T)omega, 0, nullptr)));
-            it++;
+            CKS((launch_stencil<T, OP_JACOBI>(s, l, uprev_ptr(s, l), u_ptr(s, l), (T)omega, 0, nullptr)));
         }
     } else {
         for (int64_t it = 0; it < 2 * nsmooth; it++) {
@@ -812,14 +902,21 @@ int coarse_setup_fused_t(mgp_solver* s, int l, const FirstSweep<T>& w) {
 // uses it on every level.
 constexpr long long kFusedSetupMaxPoints = 1ll << 20;
 
-template <typename T>
-int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns) {
+// The set-up of level l forms its residual in a separate pass (the three-kernel form), which
+// the relaxation before it may take over.
+bool setup_residual_separate(const mgp_solver* s, int l) {
     const Geom& G = s->lv[l].G;
+    return !((s->desc.flags & MGP_FLAG_FUSED_SETUP) || (long long)G.nx * G.ny * G.nz <= kFusedSetupMaxPoints);
+}
+
+// resid_done: the relaxation before the set-up already stored r (wavefront pass).
+template <typename T>
+int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns, bool resid_done = false) {
     const FirstSweep<T> w = first_sweep_of<T>(s, l, omega, ns);
-    if ((s->desc.flags & MGP_FLAG_FUSED_SETUP) || (long long)G.nx * G.ny * G.nz <= kFusedSetupMaxPoints) {
+    if (!setup_residual_separate(s, l)) {
         CKS(coarse_setup_fused_t<T>(s, l, w));
     } else {
-        CKS(residual_t<T>(s, l, nullptr));
+        if (!resid_done) CKS(residual_t<T>(s, l, nullptr));
         CKS(restrict_bc_t<T>(s, l));  // before the restriction: the first sweep reads the coarse faces
         CKS(restrict_t<T>(s, l, /*zero_coarse_u=*/true, w));
     }
@@ -827,27 +924,37 @@ int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns) {
     return MGP_OK;
 }
 
+// tail_norm: the caller's residual of level l with its max-norm, right after this cycle (the
+// solve loop's); the cycle's last relaxation may take it over and then sets *tail_done.
 template <typename T>
-int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
+int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns, unsigned long long* tail_norm = nullptr,
+             bool* tail_done = nullptr) {
     // Vcycle<T> (include/vcycle.h:14-98)
-    CKS(relax_t<T>(s, l, omega, ns, /*later=*/l < s->levels - 1));
-    if (l >= s->levels - 1) return MGP_OK;
-    CKS(coarse_setup_t<T>(s, l, omega, ns));
+    const int tail = tail_norm ? RESID_NORM : RESID_NONE;
+    if (l >= s->levels - 1) return relax_t<T>(s, l, omega, ns, false, tail, tail_norm, tail_done);
+    bool rd = false;
+    CKS(relax_t<T>(s, l, omega, ns, /*later=*/true, setup_residual_separate(s, l) ? RESID_STORE : RESID_NONE, nullptr,
+                   &rd));
+    CKS(coarse_setup_t<T>(s, l, omega, ns, rd));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
     CKS((prolong_t<T, true>(s, l)));
-    CKS(relax_t<T>(s, l, omega, ns));
+    CKS(relax_t<T>(s, l, omega, ns, false, tail, tail_norm, tail_done));
     return MGP_OK;
 }
 
 template <typename T>
-int fcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
+int fcycle_t(mgp_solver* s, int l, double omega, int64_t ns, unsigned long long* tail_norm = nullptr,
+             bool* tail_done = nullptr) {
     // Fcycle<T> (include/fcycle.h:13-97); the V-cycle of this level that follows relaxes it again
-    CKS(relax_t<T>(s, l, omega, ns, /*later=*/true));
-    CKS(coarse_setup_t<T>(s, l, omega, ns));
+    if (tail_done) *tail_done = false;
+    bool rd = false;
+    CKS(relax_t<T>(s, l, omega, ns, /*later=*/true, setup_residual_separate(s, l) ? RESID_STORE : RESID_NONE, nullptr,
+                   &rd));
+    CKS(coarse_setup_t<T>(s, l, omega, ns, rd));
     if (l < s->levels - 2) CKS(fcycle_t<T>(s, l + 1, omega, ns));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
     CKS((prolong_t<T, true>(s, l)));
-    if (l == 0) CKS(vcycle_t<T>(s, 0, omega, ns));
+    if (l == 0) CKS(vcycle_t<T>(s, 0, omega, ns, tail_norm, tail_done));
     return MGP_OK;
 }
 
@@ -859,10 +966,12 @@ int fcycle_t(mgp_solver* s, int l, double omega, int64_t ns) {
 // One solve iteration: the cycle, then residual + max-norm of the finest level
 // (include/libpoisson.h:294-330).  Captured once per (cycle, nsmooth, omega, state).
 int iteration_body(mgp_solver* s, int cycle, int64_t ns, double omega) {
-    if (cycle == MGP_CYCLE_V) CKS(DISPATCH(s, (vcycle_t<T>(s, 0, omega, ns))));
-    else if (cycle == MGP_CYCLE_F) CKS(DISPATCH(s, (fcycle_t<T>(s, 0, omega, ns))));
+    // the norm word is zeroed first: the cycle's last pass may already reduce into it
     CK(cudaMemsetAsync(s->d_norm, 0, sizeof(unsigned long long), s->stream));
-    CKS(DISPATCH(s, (residual_t<T>(s, 0, s->d_norm))));
+    bool done = false;
+    if (cycle == MGP_CYCLE_V) CKS(DISPATCH(s, (vcycle_t<T>(s, 0, omega, ns, s->d_norm, &done))));
+    else if (cycle == MGP_CYCLE_F) CKS(DISPATCH(s, (fcycle_t<T>(s, 0, omega, ns, s->d_norm, &done))));
+    if (!done) CKS(DISPATCH(s, (residual_t<T>(s, 0, s->d_norm))));
     return MGP_OK;
 }
 
@@ -906,13 +1015,13 @@ int launch_iteration(mgp_solver* s, int cycle, int64_t ns, double omega) {
 }
 
 int read_norm(mgp_solver* s, double* out) {
-    // the norm word and, 8 bytes on, the error word of the TMA-fed sweeps
+    // the norm word and, 8 bytes on, the error word of the wavefront passes
     CK(cudaMemcpyAsync(s->h_norm, s->d_norm, 16, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     if (reinterpret_cast<const int*>(s->h_norm)[2]) {
         CK(cudaMemsetAsync(s->err_word, 0, sizeof(int), s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        return fail(MGP_ERR_TIMEOUT, "stencil sweep: a shared-memory ring wait ran out of time; results are invalid");
+        return fail(MGP_ERR_TIMEOUT, "wavefront pass: a shared-memory ring wait ran out of time; results are invalid");
     }
     double v;
     unsigned long long b = *s->h_norm;
@@ -1341,18 +1450,14 @@ static int create_plain(const mgp_desc* d, mgp_solver** out, const CreateCtx* ct
     }
     for (int l = 0; l < s->levels; l++)
         s->lv[l].G.poff = s->lv[l].gs_column ? (int)((hs + hb) & 1) : (int)((hw + hs + hb) & 1);
-    for (int l = 0; l < s->levels; l++) {
-        if (s->dtype == MGP_F64) tma_prepare_level<double>(s, s->lv[l]);
-        else tma_prepare_level<float>(s, s->lv[l]);
-    }
     {
         int npair = 0;
         for (int l = 0; l < s->levels; l++) {
-            cudaError_t e = s->dtype == MGP_F64 ? pair_prepare_level<double>(s, s->lv[l], npair)
-                                                : pair_prepare_level<float>(s, s->lv[l], npair);
+            cudaError_t e = s->dtype == MGP_F64 ? wave_prepare_level<double>(s, s->lv[l], npair)
+                                                : wave_prepare_level<float>(s, s->lv[l], npair);
             if (e != cudaSuccess) {
                 release(s);
-                return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "sweep-pair buffer of level %d: %s",
+                return fail(e == cudaErrorMemoryAllocation ? MGP_ERR_OOM : MGP_ERR_CUDA, "wavefront buffer of level %d: %s",
                             l, cudaGetErrorString(e));
             }
             npair += s->lv[l].pair;
@@ -1514,6 +1619,23 @@ int mgp_write_bc(mgp_solver* s, int l) {
     return MGP_OK;
 }
 
+int mgp_set_wait_polls(mgp_solver* s, int64_t polls) {
+    CKS(validate(s));
+    if (polls < 0 || polls > (int64_t)UINT32_MAX) return fail(MGP_ERR_INVALID_ARG, "polls must be in [0, 2^32)");
+    const unsigned p = polls == 0 ? kWaitPolls : (unsigned)polls;
+    DeviceGuard guard(s->device);
+    CK(cudaStreamSynchronize(s->stream));
+    // the captured iterations carry the bound in their kernels' parameters
+    for (mgp_solver* x : {s, s->inner}) {
+        if (!x) continue;
+        x->wait_polls = p;
+        for (auto& kv : x->graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        x->graphs.clear();
+    }
+    return MGP_OK;
+}
+
 int mgp_set_iteration_limits(mgp_solver* s, int64_t maxiter, int64_t miniter, double tolerance) {
     CKS(validate(s));
     s->desc.maxiter = maxiter;
@@ -1528,6 +1650,18 @@ int mgp_relax(mgp_solver* s, int l, double omega, int64_t nsmooth) {
     DeviceGuard guard(s->device);
     if (omega < 0) omega = s->desc.relaxation == MGP_JACOBI ? 6.0 / 7.0 : 8.0 / 9.0;
     return DISPATCH(s, (relax_t<T>(s, l, omega, nsmooth)));
+}
+int mgp_relax_residual(mgp_solver* s, int l, double omega, int64_t nsmooth, double* norm) {
+    CKS(validate_level(s, l));
+    DeviceGuard guard(s->device);
+    if (omega < 0) omega = s->desc.relaxation == MGP_JACOBI ? 6.0 / 7.0 : 8.0 / 9.0;
+    unsigned long long* nw = norm ? s->d_norm : nullptr;
+    if (nw) CK(cudaMemsetAsync(s->d_norm, 0, sizeof(unsigned long long), s->stream));
+    bool done = false;
+    CKS(DISPATCH(s, (relax_t<T>(s, l, omega, nsmooth, false, nw ? RESID_NORM : RESID_STORE, nw, &done))));
+    if (!done) CKS(DISPATCH(s, (residual_t<T>(s, l, nw))));
+    if (nw) return read_norm(s, norm);
+    return MGP_OK;
 }
 int mgp_residual(mgp_solver* s, int l) {
     CKS(validate_level(s, l));

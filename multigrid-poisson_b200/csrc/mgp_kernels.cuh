@@ -207,6 +207,25 @@ __device__ __forceinline__ void lds_v(T (&d)[VecT<T>::V], const T* p) {
 
 constexpr int kStages = 4;  // planes of u and f in flight per thread
 
+// Position t of a plane's ny x nv vectors -> row j and vector kv: the interior vectors
+// (kv = 1 .. nv-2) of every row first, row by row, then the two end vectors of every row.  The
+// warps of interior vectors then hold no vector on a k face, so on interior rows and planes
+// they all take the condition-free stencil together.
+__device__ __forceinline__ void plane_vector(int t, int ny, int nv, int& j, int& kv) {
+    const int ni = nv - 2;
+    if (ni < 1) {
+        j = t / nv;
+        kv = t - j * nv;
+    } else if (t < ny * ni) {
+        j = t / ni;
+        kv = 1 + t - j * ni;
+    } else {
+        const int q = t - ny * ni;
+        j = q >> 1;
+        kv = (q & 1) ? nv - 1 : 0;
+    }
+}
+
 // One thread owns a V-vector of k points of one (j) row and marches i over a chunk of
 // planes with u(i-1), u(i), u(i+1) in registers.  The next kStages planes of u and f are
 // staged by cp.async into the thread's own shared-memory slots, so each thread keeps
@@ -226,10 +245,14 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
     const int ib = min(G.nx, ia + a.ichunk);
     unsigned long long mx = 0ull;
     if (t < G.ny * nv) {
-        const int j = t / nv;
-        const int kb = (t - j * nv) * V;
+        int j, kv;
+        plane_vector(t, G.ny, nv, j, kv);
+        const int kb = kv * V;
         const long long bjk = (long long)j * G.sy + kb;
         const bool jin = j >= G.y0 && j < G.y1;
+        // every point of the vector relaxed and off the face lines (on an interior plane): no
+        // ghosts, no masks (column-ordered Gauss-Seidel keeps the general body)
+        const bool fast = OP != OP_GS_COLUMN && nv >= 3 && kv >= 1 && kv <= nv - 2 && j >= 1 && j <= G.ny - 2;
         unsigned ins = 0u, inr = 0u;  // elements inside the shape / inside the relaxation bounds
 #pragma unroll
         for (int e = 0; e < V; e++) {
@@ -281,6 +304,47 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
             for (int i = i0; i < i1; i++) {
                 const long long p = (long long)i * G.sx + bjk;
                 const int slot = (i - i0) % kStages;
+                if (fast && i >= 1 && i + 1 < G.nx) {
+                    // the condition-free body: every neighbour is a point of the level
+                    cp_async_wait<kStages - 1>();
+                    lds_v(vp, su + slot * SS);
+                    lds_v(fc, sf + slot * SS);
+                    {
+                        const int q = i + kStages;
+                        if (q < i1) {
+                            if (q + 1 < G.nx) cp_async16(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
+                            cp_async16(sf + slot * SS, f + (long long)q * G.sx + bjk);
+                        }
+                        cp_async_commit();
+                    }
+                    T ym[V], yp[V], cur[V];
+                    ldv(ym, src + p - G.sy);
+                    ldv(yp, src + p + G.sy);
+                    const T left = ldg(src + p - 1), right = ldg(src + p + V);
+                    const int base = i + j + kb + G.poff;  // red-black colour of element 0
+#pragma unroll
+                    for (int e = 0; e < V; e++) {
+                        const T below = e > 0 ? vc[e - 1] : left;
+                        const T above = e < V - 1 ? vc[e + 1] : right;
+                        const T sum = vm[e] + vp[e] + ym[e] + yp[e] + below + above;
+                        if (OP == OP_RESIDUAL) {
+                            const T r = residual_pt(fc[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
+                            cur[e] = r;
+                            if (NORM) mx = max(mx, abs_bits(r));
+                        } else {
+                            const T v = a.one_omega * vc[e] + a.omega_sixth * (sum - a.hsq * fc[e]);
+                            cur[e] = (OP == OP_GS && ((base + e) & 1) != a.colour) ? vc[e] : v;
+                        }
+                    }
+                    stv(a.dst + p, cur);
+#pragma unroll
+                    for (int e = 0; e < V; e++) {
+                        vmo[e] = vc[e];
+                        vm[e] = OP == OP_GS ? cur[e] : vc[e];
+                        vc[e] = vp[e];
+                    }
+                    continue;
+                }
                 cp_async_wait<kStages - 1>();
                 if (i + 1 < G.nx) {
                     lds_v(vp, su + slot * SS);

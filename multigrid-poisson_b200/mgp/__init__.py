@@ -39,8 +39,7 @@ FLAG_STRICT_BC = 1
 FLAG_FUSED_SETUP = 8
 FLAG_REFINE_F32 = 16
 FLAG_REFINE_F64 = 32
-FLAG_TMA_SWEEPS = 64
-FLAG_SWEEP_PAIRS = 128
+FLAG_WAVE = 256
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,
@@ -114,6 +113,8 @@ def lib():
         L.mgp_solve.argtypes = [vp, i32, i64, dbl, ctypes.c_char_p, dbl, ctypes.c_uint32, ctypes.POINTER(Stats)]
         L.mgp_set_iteration_limits.argtypes = [vp, i64, i64, dbl]
         L.mgp_relax.argtypes = [vp, i32, dbl, i64]
+        L.mgp_set_wait_polls.argtypes = [vp, i64]
+        L.mgp_relax_residual.argtypes = [vp, i32, dbl, i64, ctypes.POINTER(ctypes.c_double)]
         for n in ("mgp_residual", "mgp_restrict", "mgp_zero_u", "mgp_restrict_bc", "mgp_prolong", "mgp_add",
                   "mgp_prolong_add"):
             getattr(L, n).argtypes = [vp, i32]
@@ -328,6 +329,16 @@ class Solver:
     # ---- operators ----
     def relax(self, level, omega=-1.0, nsmooth=1):
         _check(lib().mgp_relax(self._h, level, omega, nsmooth))
+
+    def set_wait_polls(self, polls):
+        """Bound of the wavefront passes' waits for a plane copy (0: the default)."""
+        _check(lib().mgp_set_wait_polls(self._h, polls))
+
+    def relax_residual(self, level, omega=-1.0, nsmooth=1, norm=True):
+        """relax, then residual (and the max-norm of r when `norm`): returns the norm or None."""
+        out = ctypes.c_double()
+        _check(lib().mgp_relax_residual(self._h, level, omega, nsmooth, ctypes.byref(out) if norm else None))
+        return out.value if norm else None
 
     def residual(self, level):
         _check(lib().mgp_residual(self._h, level))
