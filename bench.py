@@ -239,7 +239,13 @@ def run_kernels(args):
         # two sweeps and the residual with its max-norm in one pass: read u, f; write u2, u1, r
         "pair_residual_norm": (lambda: eng.relax_residual(0, -1.0, 2, norm=True), 40.0 * n),
         "residual": (lambda: eng.residual(0), 24.0 * n),
+        # the solve loop's residual with its max-norm (and the norm's read-back): read u, f; write r
+        "residual_norm": (lambda: eng.relax_residual(0, -1.0, 0, norm=True), 24.0 * n),
         "restrict_fw": (lambda: eng.restrict(0), 8.0 * (n + nc)),
+        # the coarse sub-cycles inside one F-cycle iteration (F(1) once, V(1) twice), launched
+        # directly; bytes: the cycle model's share of levels 1..5
+        "fcycle_level1": (lambda: eng.fcycle(1, -1.0, NSMOOTH), 0.0),
+        "vcycle_level1": (lambda: eng.vcycle(1, -1.0, NSMOOTH), 0.0),
         "prolong_add": (lambda: eng.prolong_add(0), 8.0 * (2 * n + nc)),
     }
     peak, kind = measured_peaks()
@@ -256,7 +262,7 @@ def run_kernels(args):
         b.synchronize()
         us = a.elapsed_time(b) * 1e3 / args.steps
         gbs = nbytes / (us * 1e-6) / 1e9
-        out[name] = {"us": us, "algorithmic_bytes": nbytes, "GB/s": gbs, "frac": gbs / peak}
+        out[name] = {"us": us, "algorithmic_bytes": nbytes, "GB/s": gbs, "frac": gbs / peak} if nbytes else {"us": us}
     print(json.dumps({"kernels": out, "peak_gbs": peak, "peak_kind": kind, "workload": WORKLOAD}))
     return 0
 

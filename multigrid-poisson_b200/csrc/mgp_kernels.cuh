@@ -205,7 +205,10 @@ __device__ __forceinline__ void lds_v(T (&d)[VecT<T>::V], const T* p) {
     for (int e = 0; e < VecT<T>::V; e++) d[e] = p[e];
 }
 
-constexpr int kStages = 4;  // planes of u and f in flight per thread
+#ifndef MGP_STAGES
+#define MGP_STAGES 4
+#endif
+constexpr int kStages = MGP_STAGES;  // planes of u and f in flight per thread
 
 // Position t of a plane's ny x nv vectors -> row j and vector kv: the interior vectors
 // (kv = 1 .. nv-2) of every row first, row by row, then the two end vectors of every row.  The

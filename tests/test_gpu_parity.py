@@ -337,3 +337,40 @@ def test_fp32_engine_tracks_fp64_oracle(mgp_mod, gpu_ready):
     o.vcycle(0, o.default_omega(), 2)
     e.vcycle(0, -1.0, 2)
     assert_field_equal(o, e, "u", 0, exact=False, rtol=1e-4)
+
+
+FW_EDGES = [
+    # coarse extents even and odd in j and k, Neumann and Dirichlet faces
+    ((65, 33, 33), 2, (1, 1, 1, 1, 0, 0)),
+    ((33, 65, 17), 2, (0, 0, 1, 1, 1, 1)),
+    ((17, 9, 65), 2, (1, 0, 0, 1, 0, 1)),
+    ((129, 65, 129), 2, (1, 1, 1, 1, 0, 0)),
+]
+
+
+@pytest.mark.parametrize("ci", range(len(FW_EDGES)))
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_fullweighting_edges_bit_exact(mgp_mod, gpu_ready, ci, dtype):
+    """FullWeighting over coarse extents even and odd in j and k, on faces of every kind: f on
+    the coarse level bit-identical to the oracle (FP64), and within FP32 rounding of it (FP32)."""
+    dims, levels, bc = FW_EDGES[ci]
+    cfg = {"dims": dims, "levels": levels, "bc": bc, "restriction": "fw", "relaxation": "jacobi", "h": 1 / 64,
+           "strict_bc": True}
+    o = make_oracle(cfg)
+    randomize(o, 900 + ci)
+    if dtype == "f64":
+        e = make_engine(mgp_mod, cfg)
+        push(o, e)
+        o.restrict(0)
+        e.restrict(0)
+        assert_field_equal(o, e, "f", 1)
+    else:
+        e = make_engine(mgp_mod, cfg, dtype=mgp_mod.F32)
+        for l in range(o.levels):
+            for name in ("u", "uprev", "f", "r"):
+                o.field(name, l)[...] = o.field(name, l).astype(np.float32)
+                e.upload(name, o.field(name, l).astype(np.float32), l)
+        o.restrict(0)
+        e.restrict(0)
+        assert_field_equal(o, e, "f", 1, exact=False, rtol=1e-6)
+    e.close()
