@@ -530,6 +530,24 @@ def run_reference_arm(args):
     return 0
 
 
+def run_iterations_only(args) -> int:
+    """The workload's solve iterations and nothing else (no timing, no other workloads): the
+    command that ncu launch lists are taken from."""
+    import torch
+
+    import mgp
+
+    torch.cuda.set_device(0)
+    ps = build_solver(mgp, 0, maxiter=max(1, args.warmup + args.steps), pinned=False, flags=args.engine_flags)
+    ps.to_device()
+    eng = ps.engine
+    eng.set_iteration_limits(args.warmup + args.steps, args.warmup + args.steps, 0.0)
+    st = eng.solve("Fcycle", NSMOOTH)
+    torch.cuda.synchronize()
+    print(json.dumps({"iterations": st.cycles_run, "kernel_launches": st.kernel_launches, "rel_res": st.rel_res}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -541,13 +559,19 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the mixed-precision, batched and served workloads")
     ap.add_argument("--served-requests", type=int, default=120)
+    ap.add_argument("--iterations-only", action="store_true",
+                    help="run --warmup + --steps solve iterations of the workload and exit (for ncu launch lists)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the built-in launch shapes (no mgp_autotune search before timing)")
     ap.add_argument("--engine-flags", type=int, default=0,
-                    help="extra MGP_FLAG_* bits for the benchmarked solver (e.g. 64: TMA-fed sweeps)")
+                    help="extra MGP_FLAG_* bits for the benchmarked solver (e.g. 256: wavefront passes)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.kernels:
         return run_kernels(args)
+    if args.iterations_only:
+        return run_iterations_only(args)
 
     world, rank, local, pg = dist_setup(args.gpus)
     import torch
@@ -559,6 +583,12 @@ def main():
     ps = build_solver(mgp, local, maxiter=args.steps, pinned=True, flags=args.engine_flags)
     ps.to_device()
     eng = ps.engine
+    tuning = None
+    if not args.no_tune:
+        # launch shapes searched on this GPU (fields restored afterwards); bit-identical results
+        t0 = time.time()
+        tuning = eng.autotune("Fcycle", NSMOOTH, force=True)
+        tuning["search_s"] = time.time() - t0
     stream = torch.cuda.ExternalStream(eng.stream_handle, device=f"cuda:{local}")
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -642,6 +672,12 @@ def main():
         "clocks": clocks,
         "rel_res_after": st.rel_res,
     }
+    if tuning is not None:
+        line["tuning"] = {"untuned_ms_per_iteration": tuning["untuned_ms"], "tuned_ms_per_iteration": tuning["tuned_ms"],
+                          "search_s": tuning["search_s"],
+                          "params_per_level": {"order": ["relax_planes", "resid_planes", "norm_planes", "setup_form",
+                                                         "setup_planes", "wave_off"],
+                                               "values": tuning["params"]}}
     if not args.no_extra:
         for key, fn in (("mixed_precision", lambda: bench_mixed(mgp, torch, local)),
                         ("batched", lambda: bench_batched(mgp, torch, local)),

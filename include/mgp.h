@@ -231,6 +231,32 @@ int mgp_vcycle(mgp_solver* s, int level, double omega, int64_t nsmooth);
 int mgp_fcycle(mgp_solver* s, int level, double omega, int64_t nsmooth);
 /* DeviceArray<T>::infinity_norm (include/devicearray.h:198-240), returned as double. */
 int mgp_norm(mgp_solver* s, int field, int level, double* out);
+/* ---- launch-shape tuning (no counterpart in the reference, whose OpenMP target regions
+ * take the runtime's teams) ----
+ * Per level: how the kernels of that level cut their work.  None of these changes any
+ * value a kernel computes or the order of its arithmetic: results stay bit-identical. */
+#define MGP_TUNE_RELAX_PLANES 0 /* planes marched per block by the relaxation (0 = built-in choice) */
+#define MGP_TUNE_RESID_PLANES 1 /* planes per block of the residual */
+#define MGP_TUNE_NORM_PLANES 2  /* planes per block of the residual + max-norm (solve loop) */
+#define MGP_TUNE_SETUP_FORM 3   /* coarse-grid set-up of this level: 0 built-in, 1 three kernels, 2 one kernel */
+#define MGP_TUNE_SETUP_PLANES 4 /* coarse planes per block of the one-kernel set-up (0 = built-in) */
+#define MGP_TUNE_WAVE 5         /* 0 built-in (wavefront passes where MGP_FLAG_WAVE prepared them), 1 off */
+#define MGP_TUNE_PARAMS 6
+int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value);
+int mgp_get_tuning(mgp_solver* s, int level, int param, int64_t* value);
+#define MGP_AUTOTUNE_FORCE 1u /* search again even when the process cache holds this configuration */
+/* Searches the parameters above, level by level (coordinate descent), for the fastest solve
+ * iteration of (cycle, nsmooth, omega) -- the captured graph of mgp_solve's loop body, timed
+ * with CUDA events -- and keeps them on the solver.  Refinement solvers tune their correction
+ * hierarchy.  Every field is saved to a device copy first and restored afterwards (needs that
+ * much free device memory; MGP_ERR_OOM otherwise).  Results are cached per process
+ * by (device, dtype, geometry, boundary kinds, operators, cycle, nsmooth, flags); set
+ * MGP_TUNE_CACHE to a file name to keep them across processes.  untuned_ms / tuned_ms (either
+ * may be NULL): one iteration with the built-in choices and with the tuned ones, measured
+ * after a search (0 when the cache answered). */
+int mgp_autotune(mgp_solver* s, int cycle, int64_t nsmooth, double omega, uint32_t flags, double* untuned_ms,
+                 double* tuned_ms);
+
 /* Waits for all work queued on the solver's stream. */
 int mgp_synchronize(mgp_solver* s);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */

@@ -20,7 +20,9 @@
 #include <iostream>
 #include <cstdlib>
 #include <map>
+#include <mutex>
 #include <new>
+#include <sstream>
 #include <string>
 #include <tuple>
 #include <utility>
@@ -102,6 +104,7 @@ struct LevelState {
     CUtensorMap wmap_f[4];
     CUtensorMap wmap_bk[4][3];  // u_prev's k = 0 / nz-1 columns (V x rows boxes), per allocation
     CUtensorMap wmap_bj[3];     // u_prev's j = 0 / ny-1 rows (P x 1 boxes), per allocation
+    int tune[MGP_TUNE_PARAMS] = {};  // launch shapes of this level's kernels (MGP_TUNE_*; 0 = built-in)
 };
 
 struct GraphEntry {
@@ -600,9 +603,15 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     int chunks = 1;
     if (OP != OP_GS_COLUMN) {
         const bool nrm = OP == OP_RESIDUAL && norm;
-        const int cap = sm_count(s->device) *
-                        (nrm ? resident_blocks(k_stencil<T, OP, true>) : resident_blocks(k_stencil<T, OP, false>));
-        chunks = march_chunks(bx, L.G.nx, cap);
+        const int planes = L.tune[OP == OP_RESIDUAL ? (nrm ? MGP_TUNE_NORM_PLANES : MGP_TUNE_RESID_PLANES)
+                                                    : MGP_TUNE_RELAX_PLANES];
+        if (planes > 0) {
+            chunks = (L.G.nx + planes - 1) / planes;
+        } else {
+            const int cap = sm_count(s->device) *
+                            (nrm ? resident_blocks(k_stencil<T, OP, true>) : resident_blocks(k_stencil<T, OP, false>));
+            chunks = march_chunks(bx, L.G.nx, cap);
+        }
     }
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
@@ -636,7 +645,7 @@ int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth, bool later = fa
             L.cur ^= 1;  // that sweep's swap_u
             it = 1;
         }
-        if (L.wave) {
+        if (L.wave && L.tune[MGP_TUNE_WAVE] != 1) {
             // the fused residual multiplies by 1/h^2, which is exact where h^2 is a power of two
             T hsq = (T)(L.h * L.h), inv;
             int pow2 = 0;
@@ -874,7 +883,8 @@ int coarse_setup_fused_t(mgp_solver* s, int l, const FirstSweep<T>& w) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resid_restrict<T>, tkv * rows, smem) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
-    const int chunks = march_chunks(tiles, C.G.nx, sm_count(s->device) * per_sm);
+    const int tuned = s->lv[l].tune[MGP_TUNE_SETUP_PLANES];
+    const int chunks = tuned > 0 ? (C.G.nx + tuned - 1) / tuned : march_chunks(tiles, C.G.nx, sm_count(s->device) * per_sm);
     a.ci = (C.G.nx + chunks - 1) / chunks;
     const int nchunks = (C.G.nx + a.ci - 1) / a.ci;
     a.main_blocks = tiles * nchunks;
@@ -906,7 +916,10 @@ constexpr long long kFusedSetupMaxPoints = 1ll << 20;
 // the relaxation before it may take over.
 bool setup_residual_separate(const mgp_solver* s, int l) {
     const Geom& G = s->lv[l].G;
-    return !((s->desc.flags & MGP_FLAG_FUSED_SETUP) || (long long)G.nx * G.ny * G.nz <= kFusedSetupMaxPoints);
+    if (s->desc.flags & MGP_FLAG_FUSED_SETUP) return false;
+    const int form = s->lv[l].tune[MGP_TUNE_SETUP_FORM];
+    if (form) return form == 1;
+    return (long long)G.nx * G.ny * G.nz > kFusedSetupMaxPoints;
 }
 
 // resid_done: the relaxation before the set-up already stored r (wavefront pass).
@@ -1736,6 +1749,299 @@ int mgp_get_stream(mgp_solver* s, void** stream) {
     CKS(validate(s));
     if (!stream) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
     *stream = (void*)s->stream;
+    return MGP_OK;
+}
+
+// ---- launch-shape tuning ------------------------------------------------------------------
+namespace {
+
+void drop_graphs(mgp_solver* s) {
+    for (auto& kv : s->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    s->graphs.clear();
+}
+
+// Process cache of searched configurations: key -> levels x MGP_TUNE_PARAMS values.
+std::mutex g_tune_mu;
+std::map<std::string, std::vector<int>> g_tune_cache;
+bool g_tune_file_loaded = false;
+
+const char* tune_file() {
+    const char* p = std::getenv("MGP_TUNE_CACHE");
+    return p && p[0] ? p : nullptr;
+}
+
+// One line per configuration: the key, then the values.
+void tune_cache_load_locked() {
+    if (g_tune_file_loaded) return;
+    g_tune_file_loaded = true;
+    const char* path = tune_file();
+    if (!path) return;
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ls(line);
+        std::string key;
+        if (!(ls >> key)) continue;
+        std::vector<int> v;
+        int x;
+        while (ls >> x) v.push_back(x);
+        g_tune_cache[key] = v;
+    }
+}
+
+std::string tune_key(const mgp_solver* s, int cycle, int64_t ns, uint32_t flags_used) {
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, s->device);
+    std::ostringstream k;
+    k << "sm" << p.major << p.minor << "x" << p.multiProcessorCount << "/" << (s->dtype == MGP_F64 ? "f64" : "f32")
+      << "/" << s->desc.dims[0] << "x" << s->desc.dims[1] << "x" << s->desc.dims[2] << "/L" << s->levels << "/bc";
+    for (int f = 0; f < 6; f++) k << s->face_kind[f];
+    k << "/r" << s->desc.relaxation << "p" << s->desc.prolongation << "q" << s->desc.restriction << "/c" << cycle
+      << "n" << ns << "/f" << flags_used;
+    return k.str();
+}
+
+void apply_tuning(mgp_solver* s, const std::vector<int>& v) {
+    for (int l = 0; l < s->levels; l++)
+        for (int p = 0; p < MGP_TUNE_PARAMS; p++) s->lv[l].tune[p] = v[(size_t)l * MGP_TUNE_PARAMS + p];
+    drop_graphs(s);
+}
+
+std::vector<int> current_tuning(const mgp_solver* s) {
+    std::vector<int> v((size_t)s->levels * MGP_TUNE_PARAMS);
+    for (int l = 0; l < s->levels; l++)
+        for (int p = 0; p < MGP_TUNE_PARAMS; p++) v[(size_t)l * MGP_TUNE_PARAMS + p] = s->lv[l].tune[p];
+    return v;
+}
+
+// Device copy of every field buffer of every level (u pair, spare, f, r) and the host state
+// that says which buffer is which.
+struct SavedFields {
+    void* buf = nullptr;
+    uint64_t bits = 0;
+    std::vector<std::pair<void*, size_t>> parts;  // (buffer, bytes), in copy order
+};
+
+int save_fields(mgp_solver* s, SavedFields& sv) {
+    size_t total = 0;
+    for (auto& L : s->lv)
+        for (void* p : {L.phys[0] ? L.phys[0] : L.ubuf[0], L.phys[0] ? L.phys[1] : L.ubuf[1], L.phys[2], L.f, L.r})
+            if (p) {
+                sv.parts.emplace_back(p, L.elems * s->esize);
+                total += L.elems * s->esize;
+            }
+    size_t free_b = 0, tot_b = 0;
+    CK(cudaMemGetInfo(&free_b, &tot_b));
+    if (total + (64u << 20) > free_b)
+        return fail(MGP_ERR_OOM, "autotune: %zu bytes needed for the saved fields, %zu free", total, free_b);
+    CK(cudaMalloc(&sv.buf, total));
+    size_t off = 0;
+    for (auto& pr : sv.parts) {
+        CK(cudaMemcpyAsync((char*)sv.buf + off, pr.first, pr.second, cudaMemcpyDeviceToDevice, s->stream));
+        off += pr.second;
+    }
+    sv.bits = state_bits(s);
+    return MGP_OK;
+}
+
+int restore_fields(mgp_solver* s, SavedFields& sv) {
+    size_t off = 0;
+    for (auto& pr : sv.parts) {
+        CK(cudaMemcpyAsync(pr.first, (char*)sv.buf + off, pr.second, cudaMemcpyDeviceToDevice, s->stream));
+        off += pr.second;
+    }
+    set_state_bits(s, sv.bits);
+    for (auto& L : s->lv) L.first_done = false;
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaFree(sv.buf));
+    sv.buf = nullptr;
+    return MGP_OK;
+}
+
+// Milliseconds per solve iteration of the current tuning: graphs captured afresh, two
+// iterations to warm up, then the best of `trials` runs of `reps` iterations.
+int time_iteration(mgp_solver* s, int cycle, int64_t ns, double omega, int reps, int trials, cudaEvent_t e0,
+                   cudaEvent_t e1, double* ms) {
+    drop_graphs(s);
+    for (int i = 0; i < 2; i++) CKS(launch_iteration(s, cycle, ns, omega));
+    double best = 1e30;
+    for (int t = 0; t < trials; t++) {
+        CK(cudaEventRecord(e0, s->stream));
+        for (int i = 0; i < reps; i++) CKS(launch_iteration(s, cycle, ns, omega));
+        CK(cudaEventRecord(e1, s->stream));
+        CK(cudaEventSynchronize(e1));
+        float t_ms = 0.f;
+        CK(cudaEventElapsedTime(&t_ms, e0, e1));
+        best = std::min(best, (double)t_ms / reps);
+    }
+    CK(cudaGetLastError());
+    *ms = best;
+    return MGP_OK;
+}
+
+// Coordinate descent over the levels' parameters, finest level first.  A candidate replaces
+// the current value only when it is faster by more than 0.5%, so timing noise does not move
+// a choice.
+int autotune_search(mgp_solver* s, int cycle, int64_t ns, double omega, double* untuned_ms, double* tuned_ms) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto done = [&](int st) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return st;
+    };
+    // iterations per timed run: about 20 ms of work
+    double probe = 0;
+    const std::vector<int> builtin((size_t)s->levels * MGP_TUNE_PARAMS, 0);
+    apply_tuning(s, builtin);
+    int st = time_iteration(s, cycle, ns, omega, 2, 1, e0, e1, &probe);
+    if (st != MGP_OK) return done(st);
+    const int reps = (int)std::max(3.0, std::min(200.0, 20.0 / std::max(probe, 1e-3)));
+    double best = 0;
+    st = time_iteration(s, cycle, ns, omega, reps, 3, e0, e1, &best);
+    if (st != MGP_OK) return done(st);
+    const double untuned = best;
+    static const int kPlanes[] = {1, 2, 3, 4, 5, 6, 7, 8, 12, 16, 24, 32};
+    for (int l = 0; l < s->levels; l++) {
+        LevelState& L = s->lv[l];
+        const bool coarser = l < s->levels - 1;
+        for (int p = 0; p < MGP_TUNE_PARAMS; p++) {
+            std::vector<int> cand;
+            switch (p) {
+                case MGP_TUNE_RELAX_PLANES:
+                    if (L.gs_column || (L.wave && L.tune[MGP_TUNE_WAVE] != 1)) break;
+                    // fall through
+                case MGP_TUNE_RESID_PLANES:
+                    for (int c : kPlanes)
+                        if (c < L.G.nx) cand.push_back(c);
+                    break;
+                case MGP_TUNE_NORM_PLANES:
+                    if (l == 0)
+                        for (int c : kPlanes)
+                            if (c < L.G.nx) cand.push_back(c);
+                    break;
+                case MGP_TUNE_SETUP_FORM:
+                    if (coarser && !(s->desc.flags & MGP_FLAG_FUSED_SETUP)) cand = {1, 2};
+                    break;
+                case MGP_TUNE_SETUP_PLANES:
+                    if (coarser && !setup_residual_separate(s, l))
+                        for (int c : kPlanes)
+                            if (c < s->lv[l + 1].G.nx) cand.push_back(c);
+                    break;
+                case MGP_TUNE_WAVE:
+                    if (L.wave) cand = {1};
+                    break;
+            }
+            const int keep = L.tune[p];
+            int chosen = keep;
+            for (int c : cand) {
+                if (c == keep) continue;
+                L.tune[p] = c;
+                double t = 0;
+                st = time_iteration(s, cycle, ns, omega, reps, 2, e0, e1, &t);
+                if (st != MGP_OK) return done(st);
+                if (t < best * 0.995) {
+                    best = t;
+                    chosen = c;
+                }
+            }
+            L.tune[p] = chosen;
+        }
+    }
+    // final comparison, alternating the two settings
+    const std::vector<int> tuned = current_tuning(s);
+    double tu = 1e30, tt = 1e30;
+    for (int r = 0; r < 2; r++) {
+        double t = 0;
+        apply_tuning(s, builtin);
+        if ((st = time_iteration(s, cycle, ns, omega, reps, 2, e0, e1, &t)) != MGP_OK) return done(st);
+        tu = std::min(tu, t);
+        apply_tuning(s, tuned);
+        if ((st = time_iteration(s, cycle, ns, omega, reps, 2, e0, e1, &t)) != MGP_OK) return done(st);
+        tt = std::min(tt, t);
+    }
+    tu = std::min(tu, untuned);
+    if (tt > tu) {  // the search found nothing that holds up: keep the built-in choices
+        apply_tuning(s, builtin);
+        tt = tu;
+    }
+    if (untuned_ms) *untuned_ms = tu;
+    if (tuned_ms) *tuned_ms = tt;
+    return done(MGP_OK);
+}
+
+}  // namespace
+
+int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value) {
+    CKS(validate(s));
+    mgp_solver* t = s->inner ? s->inner : s;
+    if (level < 0 || level >= t->levels) return fail(MGP_ERR_INVALID_ARG, "level %d out of range", level);
+    if (param < 0 || param >= MGP_TUNE_PARAMS) return fail(MGP_ERR_INVALID_ARG, "unknown tuning parameter %d", param);
+    const int64_t hi = param == MGP_TUNE_SETUP_FORM ? 2 : param == MGP_TUNE_WAVE ? 1 : (int64_t)1 << 20;
+    if (value < 0 || value > hi) return fail(MGP_ERR_INVALID_ARG, "tuning value %lld out of range", (long long)value);
+    DeviceGuard guard(t->device);
+    CK(cudaStreamSynchronize(t->stream));
+    t->lv[level].tune[param] = (int)value;
+    drop_graphs(t);
+    return MGP_OK;
+}
+
+int mgp_get_tuning(mgp_solver* s, int level, int param, int64_t* value) {
+    CKS(validate(s));
+    const mgp_solver* t = s->inner ? s->inner : s;
+    if (!value) return fail(MGP_ERR_INVALID_ARG, "null out pointer");
+    if (level < 0 || level >= t->levels) return fail(MGP_ERR_INVALID_ARG, "level %d out of range", level);
+    if (param < 0 || param >= MGP_TUNE_PARAMS) return fail(MGP_ERR_INVALID_ARG, "unknown tuning parameter %d", param);
+    *value = t->lv[level].tune[param];
+    return MGP_OK;
+}
+
+int mgp_autotune(mgp_solver* s, int cycle, int64_t nsmooth, double omega, uint32_t flags, double* untuned_ms,
+                 double* tuned_ms) {
+    CKS(validate(s));
+    if (cycle != MGP_CYCLE_V && cycle != MGP_CYCLE_F)
+        return fail(MGP_ERR_INVALID_ARG, "autotune: cycle must be MGP_CYCLE_V or MGP_CYCLE_F");
+    if (nsmooth < 0) return fail(MGP_ERR_INVALID_ARG, "nsmooth must be >= 0");
+    mgp_solver* t = s->inner ? s->inner : s;
+    if (cycle == MGP_CYCLE_F && t->levels < 2) return fail(MGP_ERR_INVALID_ARG, "an F-cycle needs at least 2 levels");
+    DeviceGuard guard(t->device);
+    if (omega < 0) omega = t->desc.relaxation == MGP_JACOBI ? 6.0 / 7.0 : 8.0 / 9.0;
+    if (untuned_ms) *untuned_ms = 0;
+    if (tuned_ms) *tuned_ms = 0;
+    const std::string key = tune_key(t, cycle, nsmooth, t->desc.flags & (MGP_FLAG_WAVE | MGP_FLAG_FUSED_SETUP));
+    if (!(flags & MGP_AUTOTUNE_FORCE)) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_cache_load_locked();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end() && it->second.size() == (size_t)t->levels * MGP_TUNE_PARAMS) {
+            CK(cudaStreamSynchronize(t->stream));
+            apply_tuning(t, it->second);
+            return MGP_OK;
+        }
+    }
+    CK(cudaStreamSynchronize(t->stream));
+    SavedFields sv;
+    CKS(save_fields(t, sv));
+    const std::vector<int> before = current_tuning(t);
+    int st = autotune_search(t, cycle, nsmooth, omega, untuned_ms, tuned_ms);
+    const int rs = restore_fields(t, sv);
+    drop_graphs(t);
+    if (st != MGP_OK) {
+        apply_tuning(t, before);
+        return st;
+    }
+    CKS(rs);
+    const std::vector<int> v = current_tuning(t);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = v;
+    if (const char* path = tune_file()) {
+        std::ofstream out(path, std::ios::app);
+        out << key;
+        for (int x : v) out << ' ' << x;
+        out << '\n';
+    }
     return MGP_OK;
 }
 

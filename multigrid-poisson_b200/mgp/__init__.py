@@ -41,6 +41,10 @@ FLAG_REFINE_F32 = 16
 FLAG_REFINE_F64 = 32
 FLAG_WAVE = 256
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
+# launch-shape tuning parameters (mgp_set_tuning / mgp_autotune)
+TUNE_RELAX_PLANES, TUNE_RESID_PLANES, TUNE_NORM_PLANES, TUNE_SETUP_FORM, TUNE_SETUP_PLANES, TUNE_WAVE = range(6)
+TUNE_PARAMS = 6
+AUTOTUNE_FORCE = 1
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,
                  "FullWeighting": FULLWEIGHTING, "fullweighting": FULLWEIGHTING, "fw": FULLWEIGHTING}
@@ -114,6 +118,9 @@ def lib():
         L.mgp_set_iteration_limits.argtypes = [vp, i64, i64, dbl]
         L.mgp_relax.argtypes = [vp, i32, dbl, i64]
         L.mgp_set_wait_polls.argtypes = [vp, i64]
+        L.mgp_set_tuning.argtypes = [vp, i32, i32, i64]
+        L.mgp_get_tuning.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
+        L.mgp_autotune.argtypes = [vp, i32, i64, dbl, ctypes.c_uint32, ctypes.POINTER(dbl), ctypes.POINTER(dbl)]
         L.mgp_relax_residual.argtypes = [vp, i32, dbl, i64, ctypes.POINTER(ctypes.c_double)]
         for n in ("mgp_residual", "mgp_restrict", "mgp_zero_u", "mgp_restrict_bc", "mgp_prolong", "mgp_add",
                   "mgp_prolong_add"):
@@ -333,6 +340,29 @@ class Solver:
     def set_wait_polls(self, polls):
         """Bound of the wavefront passes' waits for a plane copy (0: the default)."""
         _check(lib().mgp_set_wait_polls(self._h, polls))
+
+    def set_tuning(self, level, param, value):
+        """Launch shape of one level's kernels (TUNE_*; 0 = the built-in choice)."""
+        _check(lib().mgp_set_tuning(self._h, level, param, value))
+
+    def get_tuning(self, level, param):
+        v = ctypes.c_int64()
+        _check(lib().mgp_get_tuning(self._h, level, param, ctypes.byref(v)))
+        return v.value
+
+    def tuning(self):
+        """All levels' tuning parameters: one list of TUNE_PARAMS values per level."""
+        return [[self.get_tuning(l, p) for p in range(TUNE_PARAMS)] for l in range(self.levels)]
+
+    def autotune(self, cycle="Fcycle", nsmooth=2, omega=-1.0, force=False):
+        """Searches the launch shapes for the fastest solve iteration of (cycle, nsmooth) and keeps
+        them (fields restored afterwards).  Returns {"untuned_ms", "tuned_ms", "params"}; the two
+        times are 0 when the process cache answered."""
+        cyc = cycle if isinstance(cycle, int) else _CYCLES[cycle]
+        u, t = ctypes.c_double(), ctypes.c_double()
+        _check(lib().mgp_autotune(self._h, cyc, nsmooth, omega, AUTOTUNE_FORCE if force else 0, ctypes.byref(u),
+                                  ctypes.byref(t)))
+        return {"untuned_ms": u.value, "tuned_ms": t.value, "params": self.tuning()}
 
     def relax_residual(self, level, omega=-1.0, nsmooth=1, norm=True):
         """relax, then residual (and the max-norm of r when `norm`): returns the norm or None."""
