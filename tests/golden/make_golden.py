@@ -2,7 +2,7 @@
 
 Run where the reference sources are present (they are compiled by oracle/build_ref.sh):
 
-    REF_DIR=<reference source dir> python tests/golden/make_golden.py
+    REF_DIR=<reference source dir> python tests/golden/make_golden.py [--only NAME ...]
 
 Writes ``tests/golden/solves.json`` (whole PoissonSolver::solve runs: final relative
 residual, reported iterations, and SHA-256 digests of the level-0 solution and residual
@@ -37,6 +37,8 @@ SOLVES = {
     "c2_fcycle_65": ((65, 33, 17), 4, (N, N, N, N, D, D), "fw", "jacobi", 2, "Fcycle", 2, 4, 1 / 64, (0, 0, 0), 0.0, 4),
     "c2_fcycle_full": ((513, 257, 129), 6, (N, N, N, N, D, D), "fw", "jacobi", 2, "Fcycle", 2, 2, 1 / 512, (0, 0, 0),
                        0.0, 8),
+    "c2_vcycle_full": ((513, 257, 129), 6, (N, N, N, N, D, D), "fw", "jacobi", 2, "Vcycle", 2, 3, 1 / 512, (0, 0, 0),
+                       0.0, 8),
     # cos(x z^2) sin(y^3), FW + GS converging F-cycle with the reference stopping rule active
     "c3_fcycle_33": ((33, 33, 17), 4, (D,) * 6, "fw", "gs", 3, "Fcycle", 2, 30, 1 / 32, (0, 0, 0), 1e-10, 4),
     # Neumann east/west/top with Jacobi + Injection, sin problem with the reference origin
@@ -65,9 +67,11 @@ def interior(m):
     return (slice(h["west"], h["west"] + nx), slice(h["south"], h["south"] + ny), slice(h["bottom"], h["bottom"] + nz))
 
 
-def make_solves(ref: RefRun) -> dict:
+def make_solves(ref: RefRun, only=None) -> dict:
     out = {}
     for name, (dims, levels, bc, rst, rlx, prob, cyc, ns, mi, h, org, tol, thr) in SOLVES.items():
+        if only and name not in only:
+            continue
         st = ref.run(dims, levels, bc=bc, restriction=rst, relaxation=rlx, problem=prob, mode="solve", cycle=cyc,
                      nsmooth=ns, maxiter=mi, tol=tol, h=h, origin=org, threads=thr, timeout=1800)
         m = st.meta[0]
@@ -142,8 +146,16 @@ def main():
     if binary is None or not Path(binary).exists():
         raise SystemExit("reference sources not available: cannot generate golden vectors")
     ref = RefRun(binary)
-    solves = make_solves(ref)
+    # `--only NAME ...` regenerates the named solves and keeps every other fixture as it is
+    only = sys.argv[sys.argv.index("--only") + 1:] if "--only" in sys.argv else None
+    solves = make_solves(ref, only)
+    if only:
+        kept = json.loads((HERE / "solves.json").read_text())
+        kept.update(solves)
+        solves = kept
     (HERE / "solves.json").write_text(json.dumps(solves, indent=1, sort_keys=True) + "\n")
+    if only:
+        return
     ops = make_ops(ref)
     np.savez_compressed(HERE / "ops.npz", **ops)
 

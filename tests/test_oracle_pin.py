@@ -15,7 +15,8 @@ from _util import digest, golden_cfg, load_ops, make_oracle
 from oracle.oracle import FACES, FIELDS, REF_BIN, RefRun
 
 SOLVES = json.loads((__import__("pathlib").Path(__file__).parent / "golden" / "solves.json").read_text())
-QUICK = [k for k in SOLVES if k != "c2_fcycle_full"]
+FULL = ("c2_fcycle_full", "c2_vcycle_full")
+QUICK = [k for k in SOLVES if k not in FULL]
 
 
 def run_oracle_solve(cfg):
@@ -37,8 +38,9 @@ def test_oracle_matches_reference_solve(name):
 
 
 @pytest.mark.slow
-def test_oracle_matches_reference_full_size_c2():
-    cfg = golden_cfg(SOLVES["c2_fcycle_full"])
+@pytest.mark.parametrize("name", FULL)
+def test_oracle_matches_reference_full_size_c2(name):
+    cfg = golden_cfg(SOLVES[name])
     o, rr, it, _ = run_oracle_solve(cfg)
     assert rr == cfg["rel_res"] and it == cfg["iters"]
     assert digest(o.shape_view("u", 0)) == cfg["u_sha256"]
