@@ -5,7 +5,7 @@ solution, including second-order convergence under grid refinement."""
 import numpy as np
 import pytest
 
-from _util import make_oracle
+from _util import make_engine, make_oracle
 from oracle.oracle import problem_u
 
 pytestmark = pytest.mark.gpu
@@ -99,3 +99,75 @@ def test_refinement_keeps_second_order_accuracy(mgp_mod, gpu_ready):
         errs.append(np.max(np.abs(u - analytic(3, u.shape, cfg["h"]))))
     rates = [np.log2(errs[i] / errs[i + 1]) for i in range(len(errs) - 1)]
     assert all(1.8 < r < 2.3 for r in rates), (errs, rates)
+
+
+STEP_CASES = [
+    # (dims, levels, bc, restriction, relaxation, cycle, inner dtype)
+    ((33, 33, 17), 4, (0,) * 6, "fw", "gs", "Fcycle", "f64"),
+    ((33, 33, 17), 4, (0,) * 6, "fw", "gs", "Fcycle", "f32"),
+    ((65, 33, 17), 4, (1, 1, 1, 1, 0, 0), "fw", "jacobi", "Vcycle", "f32"),
+    ((33, 17, 17), 3, (0, 0, 1, 0, 1, 0), "inj", "jacobi", "Fcycle", "f64"),
+]
+
+
+@pytest.mark.parametrize("ci", range(len(STEP_CASES)))
+def test_refinement_step_matches_composed_step(mgp_mod, gpu_ready, ci):
+    """One refinement step (correction cycle, u += e, new FP64 residual) against the same step
+    composed from plain solvers: r0 from an FP64 residual of u0, e from
+    one correction cycle of a zero-boundary solver of the inner precision started at u = 0,
+    u1 = u0 + e at the relaxed points (numpy), r1 from an FP64 residual of u1.  u1 and r1 must
+    be bit-identical, for two steps in a row."""
+    dims, levels, bc, rst, rlx, cyc, idt = STEP_CASES[ci]
+    cfg = {"dims": dims, "levels": levels, "bc": bc, "restriction": rst, "relaxation": rlx, "h": 1.0 / (dims[0] - 1)}
+    o = make_oracle(cfg)
+    rng = np.random.default_rng(500 + ci)
+    u0 = rng.uniform(-1, 1, size=o.meta[0].pad)
+    f = rng.uniform(-1, 1, size=o.meta[0].pad)
+    faces = [rng.uniform(-1, 1, size=o.face(fc, 0).shape) for fc in range(6)]
+    flag = mgp_mod.FLAG_REFINE_F64 if idt == "f64" else mgp_mod.FLAG_REFINE_F32
+    R = make_engine(mgp_mod, cfg, maxiter=1, tol=0.0, flags=flag)
+    P = make_engine(mgp_mod, cfg)  # FP64: residuals
+    inner_dt = mgp_mod.F64 if idt == "f64" else mgp_mod.F32
+    npdt = np.float64 if idt == "f64" else np.float32
+    Q = make_engine(mgp_mod, cfg, dtype=inner_dt)  # the correction cycle, zero boundary data
+    for e in (R, P):
+        e.upload("u", u0, 0)
+        e.upload("f", f, 0)
+        for fc in range(6):
+            e.upload_face(fc, faces[fc], 0)
+        e.write_bc(0)
+    lv = R.level[0]
+    inner = lv.interior
+    # the relaxation bounds of level 0 (Dirichlet faces excluded) inside the host layout
+    fk = dict(zip(("north", "south", "east", "west", "top", "bottom"), lv.face_kind))
+    rb = tuple(slice(h + (fk[lo_f] == 0), h + n - (fk[hi_f] == 0))
+               for h, n, lo_f, hi_f in zip((lv.halo["west"], lv.halo["south"], lv.halo["bottom"]), lv.shape,
+                                           ("west", "south", "bottom"), ("east", "north", "top")))
+    ucur = P.download("u", 0)
+    for step in range(2):
+        P.upload("u", ucur, 0)
+        P.residual(0)
+        r0 = P.download("r", 0)
+        # correction: zero-guess cycle on f = (Ti) r0 over the relaxed points
+        fi = np.zeros(lv.pad, dtype=npdt)
+        fi[rb] = r0[rb].astype(npdt)
+        for l in range(levels):
+            for name in ("u", "uprev", "f", "r"):
+                if name == "uprev" and rlx != "jacobi":
+                    continue
+                Q.upload(name, np.zeros(Q.level[l].pad, dtype=npdt), l)
+        Q.upload("f", fi, 0)
+        getattr(Q, cyc.lower())(0, -1.0, 2)
+        ecorr = Q.download("u", 0)
+        ucur = ucur.copy()
+        ucur[rb] = ucur[rb] + ecorr[rb].astype(np.float64)
+        st = R.solve(cyc, 2)
+        assert st.cycles_run == 1
+        u1 = R.download("u", 0)
+        assert np.array_equal(u1[inner], ucur[inner]), f"step {step}: u differs at {np.count_nonzero(u1[inner] != ucur[inner])} points"
+        P.upload("u", ucur, 0)
+        P.residual(0)
+        r1 = P.download("r", 0)
+        assert np.array_equal(R.download("r", 0)[rb], r1[rb])
+    for e in (R, P, Q):
+        e.close()
