@@ -487,32 +487,53 @@ def bench_batched(mgp, torch, device=0, count=256, tol=1e-8):
     return out
 
 
-def bench_served(mgp, device=0, count=120, rates=(50.0, 2000.0), seed=0):
+SERVED_ARMS = (("fp64", "F64", 32), ("mixed", "F32", 32), ("fp64_serial", "F64", 1))
+
+
+def bench_served(mgp, device=0, count=120, rates=(50.0, 2000.0), seed=0, arms=SERVED_ARMS, warm_count=None):
     """Open-loop Poisson arrivals of `count` requests at each rate: boxes 2^k+1 per axis
     (k in 5..9 for x and y, 5..8 for z), Dirichlet / Neumann / mixed, 8 random sine modes,
-    tolerance 1e-8; continuous batching with admission by free HBM.  A bounded sample of the
-    10,000-request stream.  At 50/s the server keeps up with the arrivals (latency is the
-    measure); at 2000/s the requests queue up (solves/s is the server's capacity)."""
+    tolerance 1e-8; continuous batching with admission by free HBM.  By default a bounded
+    sample of the 10,000-request stream; `--served-full` runs the whole stream at 50, 200, 1000
+    and 2000 requests/s.  At 50/s the server keeps up with the arrivals (latency is the
+    measure); at 2000/s the requests queue up (solves/s is the server's capacity).
+    fp64_serial: one request on the device at a time (a queue in front of the FP64 solver)."""
     from mgp import serve
 
     out = {}
     for rate in rates:
         res = {}
-        # fp64_serial: one request on the device at a time (a queue in front of the FP64 solver)
-        for name, inner, slots in (("fp64", mgp.F64, 32), ("mixed", mgp.F32, 32), ("fp64_serial", mgp.F64, 1)):
-            srv = serve.Server(inner=inner, max_batch=slots, device=device)
-            # warm-up pass over the same stream: the memory pool, the page-locked landing
-            # buffer and the kernels' first-launch costs are paid before the measured pass
-            srv.run(serve.make_stream(count, rate, seed, kmax_z=8))
+        for name, inner, slots in arms:
+            srv = serve.Server(inner=getattr(mgp, inner), max_batch=slots, device=device)
+            # warm-up pass over (a prefix of) the same stream: the memory pool, the page-locked
+            # landing buffer and the kernels' first-launch costs are paid before the measured pass
+            srv.run(serve.make_stream(warm_count or count, rate, seed, kmax_z=8))
             reqs = serve.make_stream(count, rate, seed, kmax_z=8)  # largest box 513x513x257
             res[name] = srv.run(reqs)
             srv.close()
-        res["speedup_mixed_over_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
-        res["speedup_mixed_over_fp64_serial"] = res["mixed"]["solves_per_s"] / res["fp64_serial"]["solves_per_s"]
+        if "fp64" in res and "mixed" in res:
+            res["speedup_mixed_over_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+        if "fp64_serial" in res and "mixed" in res:
+            res["speedup_mixed_over_fp64_serial"] = res["mixed"]["solves_per_s"] / res["fp64_serial"]["solves_per_s"]
         out[f"rate_{int(rate)}"] = res
     out["workload"] = (f"{count} requests per rate, Poisson arrivals at {', '.join(str(int(r)) for r in rates)}/s, "
-                       "sides 2^k+1, tol 1e-8 (sample of the stream)")
+                       "sides 2^k+1, tol 1e-8" + (" (sample of the stream)" if count < 10000 else ""))
     return out
+
+
+def run_served_full(args) -> int:
+    """The whole served workload: 10,000 requests at each of 50, 200, 1000 and 2000 requests/s,
+    FP64 and FP32-correction servers (warm-up on a 200-request prefix).  About a quarter of an
+    hour on one B200; prints one JSON line."""
+    import torch
+
+    import mgp
+
+    torch.cuda.set_device(0)
+    res = bench_served(mgp, 0, count=10000, rates=(50.0, 200.0, 1000.0, 2000.0), arms=SERVED_ARMS[:2],
+                       warm_count=200)
+    print(json.dumps({"served_full": res}))
+    return 0
 
 
 def measured_peaks():
@@ -660,6 +681,8 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the mixed-precision, batched and served workloads")
     ap.add_argument("--served-requests", type=int, default=120)
+    ap.add_argument("--served-full", action="store_true",
+                    help="run only the whole served workload (10,000 requests at 50/200/1000/2000 per second)")
     ap.add_argument("--iterations-only", action="store_true",
                     help="run --warmup + --steps solve iterations of the workload and exit (for ncu launch lists)")
     ap.add_argument("--no-tune", action="store_true",
@@ -673,6 +696,8 @@ def main():
         return run_kernels(args)
     if args.iterations_only:
         return run_iterations_only(args)
+    if args.served_full:
+        return run_served_full(args)
 
     world, rank, local, pg = dist_setup(args.gpus)
     import torch
