@@ -681,15 +681,8 @@ int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth, bool later = fa
 template <typename T>
 int residual_t(mgp_solver* s, int l, unsigned long long* norm) {
     LevelState& L = s->lv[l];
-    CKS((launch_stencil<T, OP_RESIDUAL>(s, l, u_ptr(s, l), L.r, T(0), 0, norm)));
-    const Geom& G = L.G;
-    if (norm && (G.x0 > 0 || G.x1 < G.nx || G.y0 > 0 || G.y1 < G.ny || G.z0 > 0 || G.z1 < G.nz)) {
-        // the stored r outside the relaxation bounds counts in the norm too
-        const int rows = G.nx * G.ny;
-        return launch_k(s, k_norm_unrelaxed<T>, dim3((rows + kThreads - 1) / kThreads), dim3(kThreads), 0,
-                        (const T*)L.r, G, norm);
-    }
-    return MGP_OK;
+    // with a norm, the march also takes the stored r outside the relaxation bounds
+    return launch_stencil<T, OP_RESIDUAL>(s, l, u_ptr(s, l), L.r, T(0), 0, norm);
 }
 
 View level_view(const LevelState& L) {

@@ -266,9 +266,42 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
         const unsigned full = (1u << V) - 1u;
         const int i0 = max(ia, G.x0);
         const int i1 = inr ? min(ib, G.x1) : i0;
-        // NORM: the max over the points this march computes; the stored r outside the
-        // relaxation bounds, which also counts in the norm (infinity_norm runs over the whole
-        // shape, devicearray.h:221-237), is taken by k_norm_unrelaxed in the same reduction.
+        // NORM: the max over the points this march computes and over the stored r outside the
+        // relaxation bounds, which counts too (infinity_norm runs over the whole shape,
+        // devicearray.h:221-237): the march's own vectors' unrelaxed lanes inside it, and here
+        // the planes and rows it does not march.
+        if (NORM) {
+            if (!inr) {  // a row outside the bounds: every plane of the chunk, 4 loads in flight
+                for (int i = ia; i < ib; i += 4) {
+                    T v[4][V];
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (i + q < ib) ldv(v[q], a.dst + (long long)(i + q) * G.sx + bjk);
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (i + q < ib) {
+#pragma unroll
+                            for (int e = 0; e < V; e++)
+                                if ((ins >> e) & 1u) mx = max(mx, abs_bits(v[q][e]));
+                        }
+                }
+            } else {  // the chunk's planes outside [x0, x1): at most the first and the last
+                for (int i = ia; i < min(ib, G.x0); i++) {
+                    T v[V];
+                    ldv(v, a.dst + (long long)i * G.sx + bjk);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if ((ins >> e) & 1u) mx = max(mx, abs_bits(v[e]));
+                }
+                for (int i = max(ia, G.x1); i < ib; i++) {
+                    T v[V];
+                    ldv(v, a.dst + (long long)i * G.sx + bjk);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if ((ins >> e) & 1u) mx = max(mx, abs_bits(v[e]));
+                }
+            }
+        }
         if (i0 < i1) {
             // src may alias dst (in-place Gauss-Seidel): every value a thread reads belongs to
             // the colour this pass does not write, or to its own vector.
@@ -423,6 +456,13 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                         }
                     }
                     T* out = a.dst + p;
+                    if (NORM && (ins & ~inr)) {  // stored r at this vector's unrelaxed points
+                        T v[V];
+                        ldv(v, out);
+#pragma unroll
+                        for (int e = 0; e < V; e++)
+                            if (((ins & ~inr) >> e) & 1u) mx = max(mx, abs_bits(v[e]));
+                    }
                     if (OP == OP_GS || OP == OP_GS_COLUMN) {
                         // the whole vector is this thread's; untouched entries keep their value
                         stv(out, cur);
@@ -1062,6 +1102,30 @@ __device__ __forceinline__ void prolong_tile(const ProlongArgs<T>& a, const int 
     const int jc = t / nv;
     const int kb = (t - jc * nv) * V;  // even
     const bool i_odd_ok = 2 * ic + 1 < Gf.nx, j_odd_ok = 2 * jc + 1 < Gf.ny;
+    unsigned ins = 0u;
+#pragma unroll
+    for (int e = 0; e < V; e++)
+        if (kb + e < Gf.nz) ins |= 1u << e;
+    const unsigned full = (1u << V) - 1u;
+    // the four fine rows' u first: their loads do not wait for the coarse values
+    T uv[2][2][V];
+    bool ok[2][2];
+    long long pp[2][2];
+#pragma unroll
+    for (int ip = 0; ip < 2; ip++)
+#pragma unroll
+        for (int jp = 0; jp < 2; jp++) {
+            ok[ip][jp] = (!ip || i_odd_ok) && (!jp || j_odd_ok);
+            pp[ip][jp] = (long long)(2 * ic + ip) * Gf.sx + (long long)(2 * jc + jp) * Gf.sy + kb;
+            if (ADD && ok[ip][jp]) {
+                if (ins == full) {
+                    ldv_rw(uv[ip][jp], u + pp[ip][jp]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < V; e++) uv[ip][jp][e] = ((ins >> e) & 1u) ? u[pp[ip][jp] + e] : T(0);
+                }
+            }
+        }
     // coarse values c[a][b][q] = C(ic+a, jc+b, kb/2+q)
     T c[2][2][NQ];
 #pragma unroll
@@ -1073,22 +1137,13 @@ __device__ __forceinline__ void prolong_tile(const ProlongArgs<T>& a, const int 
                 const int x = ic + a2, y = jc + b, z = (kb >> 1) + q;
                 c[a2][b][q] = (x < Gc.nx && y < Gc.ny && z < Gc.nz) ? ldg(uc + x * Gc.sx + y * Gc.sy + z) : T(0);
             }
-    unsigned ins = 0u;
-#pragma unroll
-    for (int e = 0; e < V; e++)
-        if (kb + e < Gf.nz) ins |= 1u << e;
-    const unsigned full = (1u << V) - 1u;
-    // the four fine rows' values, all loads issued before any store
+    // the four fine rows' prolongated values
     T ev[2][2][V];
-    T uv[2][2][V];
-    bool ok[2][2];
-    long long pp[2][2];
     unsigned insd[2][2];
 #pragma unroll
     for (int ip = 0; ip < 2; ip++)
 #pragma unroll
         for (int jp = 0; jp < 2; jp++) {
-            ok[ip][jp] = (!ip || i_odd_ok) && (!jp || j_odd_ok);
             const int i = 2 * ic + ip, j = 2 * jc + jp;
             // x pass (odd i: midpoint of the two coarse planes), then y pass, per coarse z
             T yv[NQ];
@@ -1104,21 +1159,12 @@ __device__ __forceinline__ void prolong_tile(const ProlongArgs<T>& a, const int 
 #pragma unroll
             for (int e = 0; e < V; e++)
                 ev[ip][jp][e] = (e & 1) ? half_sum(yv[e >> 1], yv[(e >> 1) + 1]) : yv[e >> 1];
-            pp[ip][jp] = (long long)i * Gf.sx + (long long)j * Gf.sy + kb;
             const bool ijin = i >= Gf.x0 && i < Gf.x1 && j >= Gf.y0 && j < Gf.y1;
             unsigned inside = 0u;
 #pragma unroll
             for (int e = 0; e < V; e++)
                 if (ijin && kb + e >= Gf.z0 && kb + e < Gf.z1) inside |= 1u << e;
             insd[ip][jp] = inside;
-            if (ADD && ok[ip][jp]) {
-                if (ins == full) {
-                    ldv_rw(uv[ip][jp], u + pp[ip][jp]);
-                } else {
-#pragma unroll
-                    for (int e = 0; e < V; e++) uv[ip][jp][e] = ((ins >> e) & 1u) ? u[pp[ip][jp] + e] : T(0);
-                }
-            }
         }
 #pragma unroll
     for (int ip = 0; ip < 2; ip++)
@@ -1172,28 +1218,6 @@ __global__ void __launch_bounds__(256) k_add(T* u, const T* __restrict__ r, Geom
         const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
         u[p] = u[p] + ldg(r + p);
     }
-}
-
-// max |r| over the points outside the relaxation bounds (they keep their stored r), into the
-// same word as the residual march's max over the points inside: whole rows (i, j) outside the
-// bounds in i or j, and the k = 0 / nz-1 ends of the other rows when z has Dirichlet faces.
-// One thread per (i, j) row; grid: ((nx*ny + 255)/256).
-template <typename T>
-__global__ void __launch_bounds__(256) k_norm_unrelaxed(const T* __restrict__ r, Geom G, unsigned long long* out) {
-    pdl_begin();
-    const int t = blockIdx.x * 256 + (int)threadIdx.x;
-    unsigned long long mx = 0ull;
-    if (t < G.nx * G.ny) {
-        const int i = t / G.ny, j = t - (t / G.ny) * G.ny;
-        const T* row = r + (long long)i * G.sx + (long long)j * G.sy;
-        if (i < G.x0 || i >= G.x1 || j < G.y0 || j >= G.y1) {
-            for (int k = 0; k < G.nz; k++) mx = max(mx, abs_bits(ldg(row + k)));
-        } else {
-            for (int k = 0; k < G.z0; k++) mx = max(mx, abs_bits(ldg(row + k)));
-            for (int k = G.z1; k < G.nz; k++) mx = max(mx, abs_bits(ldg(row + k)));
-        }
-    }
-    block_max_to(mx, out);
 }
 
 // max |a| over the shape (DeviceArray::infinity_norm).  grid: ((ny*nz + 255)/256, chunks of
