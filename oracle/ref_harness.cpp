@@ -201,6 +201,7 @@ struct Runner {
     virtual void cycle(const std::string& c, long l, double omega, long nsmooth) = 0;
     virtual double default_omega() = 0;
     virtual bool duplicate() = 0;
+    virtual void set_verbose(bool on) = 0;  // PoissonSolver::verbose (include/libpoisson.h:231-234)
 };
 
 template <template <class> class R, template <class> class S>
@@ -219,6 +220,7 @@ struct RunnerT : Runner {
                double maxtime) override {
         solver.solve(cyc, nsmooth, omega, ofile, maxtime);
     }
+    void set_verbose(bool on) override { solver.verbose(on); }
     double rel_res() override { return solver.relative_residual(); }
     double iters() override { return solver.solve_iterations(); }
     double time() override { return solver.solve_time(); }
@@ -445,6 +447,7 @@ int main(int argc, char** argv) {
         } else if (s.mode == "solve") {
             R->init(s.problem < 0);
             if (!s.load.empty()) load_host(*R, 1, s.load);
+            if (s.verbose) R->set_verbose(true);  // the solve's own prints (verbose 1 keeps stdout)
             R->to_device();
             R->solve(s.cycle, s.nsmooth, s.omega, s.ofile, s.maxtime);
             R->to_host();

@@ -2,10 +2,13 @@
 one per test problem) against the reference's own builds of the same executables
 (tests/golden/drivers.json, made by tests/golden/make_driver_golden.py): stdout, the -stats
 rows and the SHA-256 of the binary VTK files of u, f and r, with wall-clock times and the
-thread count masked.  The CPU test builds the executables and checks that they fail cleanly
-without a device."""
+thread count masked; and a user program written against the facade (tests/cpp/facade_user.cpp)
+against the reference's own solver run the same way (tests/golden/facade_user.json).  The CPU
+tests build the executables and the program and check that the drivers fail cleanly without a
+device."""
 import importlib.util
 import json
+import re
 import subprocess
 import tempfile
 from pathlib import Path
@@ -50,3 +53,44 @@ def test_driver_matches_reference_executable(gpu_ready, drivers, name):
     assert got["stdout"] == case["stdout"]
     assert got["stats"] == case["stats"]
     assert got["vtk_sha256"] == case["vtk_sha256"]
+
+
+# ---- a user program written against the facade (tests/cpp/facade_user.cpp) ---------------------
+FACADE_CASE = json.loads((GOLDEN / "facade_user.json").read_text())
+
+
+@pytest.fixture(scope="module")
+def facade_user(mgp_mod, tmp_path_factory):
+    """Compiled against the facade headers and libmgp.so, as a user's code would be."""
+    b = mgp_mod._build
+    b.build()
+    exe = tmp_path_factory.mktemp("facade") / "facade_user"
+    src = Path(__file__).parent / "cpp" / "facade_user.cpp"
+    subprocess.check_call(["g++", "-std=c++17", "-O2", f"-I{b.FACADE}", f"-I{b.INCLUDE}", str(src), f"-L{b.PKG}",
+                           "-lmgp", f"-Wl,-rpath,{b.PKG}", "-o", str(exe)])
+    return exe
+
+
+def test_facade_user_program_compiles(facade_user):
+    assert facade_user.exists()
+
+
+@pytest.mark.gpu
+def test_facade_user_program_matches_reference(gpu_ready, facade_user, tmp_path):
+    """init_zero, get_rhs(0).at[idx], get_top_bc(0).arr, verbose solve with an ofile log,
+    to_host, get_solution: the solution's bits, the verbose residual lines and the log's
+    residual column equal the reference's own solver run the same way."""
+    import hashlib
+
+    import numpy as np
+
+    u_bin, log = tmp_path / "u.bin", tmp_path / "ofile.txt"
+    p = subprocess.run([str(facade_user), str(u_bin), str(log)], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    u = np.fromfile(u_bin, dtype=np.float64)
+    assert hashlib.sha256(u.tobytes()).hexdigest() == FACADE_CASE["u_sha256"]
+    verbose = [" ".join(line.split()) for line in p.stdout.splitlines() if re.match(r"^\s*\d+:", line)]
+    assert verbose == FACADE_CASE["verbose"]
+    lines = log.read_text().splitlines()
+    assert lines[0] == FACADE_CASE["ofile_header"]
+    assert [line.split()[1] for line in lines[1:]] == FACADE_CASE["ofile_rel_res"]
