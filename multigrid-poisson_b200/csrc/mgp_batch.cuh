@@ -16,6 +16,12 @@
 // problems with top >= d inside BFF(d), and only those of the enclosing set inside a V-cycle.
 // Each problem sees exactly its own F-cycle (the same operations in the same order).
 
+// Blocks per SM that one batched launch's work list is cut into (shared among its problems by
+// points); a compile-time knob.
+#ifndef MGP_BATCH_BLOCKS_PER_SM
+#define MGP_BATCH_BLOCKS_PER_SM 8
+#endif
+
 // ---- generic persistent work-list kernel -------------------------------------------------
 template <typename Args>
 struct BatchItem {
@@ -145,6 +151,8 @@ StencilArgs<T> stencil_args(mgp_solver* s, int l, const void* src, void* dst, T 
     const int bx = (plane + kThreads - 1) / kThreads;
     int chunks = 1;
     if (OP != OP_GS_COLUMN) {
+        // no short marches here: on the 256-problem batch they cost 13% (FP64 275 -> 240, FP32
+        // 447 -> 383 solves/s); the persistent work list does better with fewer, longer tiles
         chunks = std::max(1, std::min((target + bx - 1) / bx, L.G.nx));
     }
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
@@ -218,7 +226,7 @@ int build_step(mgp_batch* b, ScheduleBuilder& sb) {
     // for the whole launch.  Few problems get many short marches each; many problems get few
     // long ones, as the batch supplies the parallelism (256-problem batch on B200: 0.99 s / 0.64 s
     // per FP64 / FP32 solve against 1.06 s / 0.69 s with a fixed SMs*2 blocks per problem).
-    const double launch_blocks = (double)sm_count(b->device) * 8;
+    const double launch_blocks = (double)sm_count(b->device) * MGP_BATCH_BLOCKS_PER_SM;
     auto shares = [&](const std::vector<BatchProblem*>& set, int d) {
         std::vector<int> t(set.size());
         double tot = 0.0;

@@ -579,6 +579,26 @@ int launch_wave(mgp_solver* s, int l, int nj, int res, bool wu1, T omega, unsign
 }
 
 // ---- stencil launches -------------------------------------------------------------------
+#ifndef MGP_SHORT_MARCH
+#define MGP_SHORT_MARCH 1  // compile-time switch of the short-march rule in launch_stencil
+#endif
+constexpr long long kShortMarchMinPoints = 1ll << 22;
+
+// Large levels whose plane does not fill a wave of blocks march short chunks.  Measured on B200
+// with the autotuner (F-cycles on 513x257x129 and 257^3): 3-5 planes per block were fastest in
+// FP64 and 2-3 in FP32, against the 13-20 the fill rule gives -- FP32 most (four points per
+// 16-byte vector, so half the threads per plane); F-cycle 513x257x129 FP32 1.164 -> 1.078 ms,
+// 1025x513x257 FP32 5.90 -> 5.24 ms, FP64 1.370 -> 1.343 and 8.29 -> 8.08 ms.  Where one plane
+// already fills a wave (1025x1025x513 FP64) the long march stays: short ones cost 2.5% there.
+template <typename T>
+int short_march_chunks(const Geom& G, int bx, int cap, int chunks) {
+    constexpr int kShort = sizeof(T) == 8 ? 4 : 3;
+    if (MGP_SHORT_MARCH && bx < cap && (long long)G.nx * G.ny * G.nz >= kShortMarchMinPoints &&
+        (G.nx + chunks - 1) / chunks > kShort)
+        return (G.nx + kShort - 1) / kShort;
+    return chunks;
+}
+
 template <typename T, int OP>
 int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, int colour, unsigned long long* norm) {
     LevelState& L = s->lv[l];
@@ -611,6 +631,7 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
             const int cap = sm_count(s->device) *
                             (nrm ? resident_blocks(k_stencil<T, OP, true>) : resident_blocks(k_stencil<T, OP, false>));
             chunks = march_chunks(bx, L.G.nx, cap);
+            chunks = short_march_chunks<T>(L.G, bx, cap, chunks);
         }
     }
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
@@ -907,12 +928,15 @@ constexpr long long kFusedSetupMaxPoints = 1ll << 20;
 
 // The set-up of level l forms its residual in a separate pass (the three-kernel form), which
 // the relaxation before it may take over.
+// FP32 hierarchies use the one-kernel form only up to 2^17 points: the autotuner chose the
+// three-kernel form for their 2^18-point levels (FP32 stencils have half the threads per plane).
 bool setup_residual_separate(const mgp_solver* s, int l) {
     const Geom& G = s->lv[l].G;
     if (s->desc.flags & MGP_FLAG_FUSED_SETUP) return false;
     const int form = s->lv[l].tune[MGP_TUNE_SETUP_FORM];
     if (form) return form == 1;
-    return (long long)G.nx * G.ny * G.nz > kFusedSetupMaxPoints;
+    const long long lim = s->dtype == MGP_F32 ? kFusedSetupMaxPoints >> 3 : kFusedSetupMaxPoints;
+    return (long long)G.nx * G.ny * G.nz > lim;
 }
 
 // resid_done: the relaxation before the set-up already stored r (wavefront pass).
