@@ -504,15 +504,12 @@ struct View {
     long long s0, s1;  // k unit-stride
 };
 
-template <typename T>
-__device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j, int k) {
-    // FullWeighting::restrict_to (include/fullweighting.h:66-109): weights (1,2,1)^3/64 with
-    // indices clamped to the array; sums in the reference's order, double accumulators.
-    const int ii = min(vi.n[0] - 1, 2 * i), jj = min(vi.n[1] - 1, 2 * j), kk = min(vi.n[2] - 1, 2 * k);
-    const int im = max(0, ii - 1), ip = min(vi.n[0] - 1, ii + 1);
-    const int jm = max(0, jj - 1), jp = min(vi.n[1] - 1, jj + 1);
-    const int km = max(0, kk - 1), kp = min(vi.n[2] - 1, kk + 1);
-    auto A = [&](int x, int y, int z) -> double { return (double)ldg(in + x * vi.s0 + y * vi.s1 + z); };
+// The FullWeighting sum at one coarse point from the clamped fine indices; A(x, y, z) reads
+// fine point (x in {im, ii, ip}, y, z) as double.  Shared by the global-memory and the
+// shared-memory restrictions, so both keep the same arithmetic.
+template <typename T, typename L>
+__device__ __forceinline__ T fw_sum(const L& A, int im, int ii, int ip, int jm, int jj, int jp, int km, int kk,
+                                    int kp) {
     const double s_m = 1.0 * A(im, jm, km) + 2.0 * A(im, jj, km) + 1.0 * A(im, jp, km) + 2.0 * A(ii, jm, km) +
                        4.0 * A(ii, jj, km) + 2.0 * A(ii, jp, km) + 1.0 * A(ip, jm, km) + 2.0 * A(ip, jj, km) +
                        1.0 * A(ip, jp, km);
@@ -526,6 +523,18 @@ __device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j,
                        1.0 * A(ip, jp, kp);
     tmp = (T)((double)tmp + s_p);
     return (T)((double)tmp / 64.0);
+}
+
+template <typename T>
+__device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j, int k) {
+    // FullWeighting::restrict_to (include/fullweighting.h:66-109): weights (1,2,1)^3/64 with
+    // indices clamped to the array; sums in the reference's order, double accumulators.
+    const int ii = min(vi.n[0] - 1, 2 * i), jj = min(vi.n[1] - 1, 2 * j), kk = min(vi.n[2] - 1, 2 * k);
+    const int im = max(0, ii - 1), ip = min(vi.n[0] - 1, ii + 1);
+    const int jm = max(0, jj - 1), jp = min(vi.n[1] - 1, jj + 1);
+    const int km = max(0, kk - 1), kp = min(vi.n[2] - 1, kk + 1);
+    auto A = [&](int x, int y, int z) -> double { return (double)ldg(in + x * vi.s0 + y * vi.s1 + z); };
+    return fw_sum<T>(A, im, ii, ip, jm, jj, jp, km, kk, kp);
 }
 
 template <typename T>
