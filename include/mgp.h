@@ -241,7 +241,10 @@ int mgp_norm(mgp_solver* s, int field, int level, double* out);
 #define MGP_TUNE_SETUP_FORM 3   /* coarse-grid set-up of this level: 0 built-in, 1 three kernels, 2 one kernel */
 #define MGP_TUNE_SETUP_PLANES 4 /* coarse planes per block of the one-kernel set-up (0 = built-in) */
 #define MGP_TUNE_WAVE 5         /* 0 built-in (wavefront passes where MGP_FLAG_WAVE prepared them), 1 off */
-#define MGP_TUNE_PARAMS 6
+#define MGP_TUNE_TAIL 6         /* level 0 only: 1 runs each cycle visit of the coarsest levels that fit in one
+                                   CTA's shared memory as one launch of one block; 0 (built-in) keeps the
+                                   grid kernels, which are faster on B200 for the 513x257x129 hierarchy */
+#define MGP_TUNE_PARAMS 7
 int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value);
 int mgp_get_tuning(mgp_solver* s, int level, int param, int64_t* value);
 #define MGP_AUTOTUNE_FORCE 1u /* search again even when the process cache holds this configuration */

@@ -31,6 +31,7 @@
 #include "mgp.h"
 #include "mgp_kernels.cuh"
 #include "mgp_wave.cuh"
+#include "mgp_tail.cuh"
 
 using namespace mgp;
 
@@ -954,12 +955,143 @@ int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns, bool resid_do
     return MGP_OK;
 }
 
+// ---- the coarsest levels in one CTA (mgp_tail.cuh) -------------------------------------
+constexpr size_t kTailMaxSmem = 220 * 1024;
+
+size_t tail_level_bytes(const mgp_solver* s, int l) {
+    const LevelState& L = s->lv[l];
+    const size_t n = (size_t)L.G.nx * L.G.ny * L.G.nz;
+    size_t faces = 0;
+    for (int f = 0; f < 6; f++) faces += (size_t)(L.face_shape[f][0] * L.face_shape[f][1] * L.face_shape[f][2]);
+    const int fields = s->desc.relaxation == MGP_JACOBI ? 4 : 3;
+    return (fields * n + faces) * s->esize;
+}
+
+// First level of the tail (0: none, the default): the smallest l >= 1 whose levels l..L-1 all
+// fit.  Not for column-ordered Gauss-Seidel layouts (their sweep order runs along i) nor for
+// levels whose Jacobi buffers rotate with a third one.  Off unless MGP_TUNE_TAIL asks for it:
+// on B200 the 513x257x129 F-cycle iteration takes 1.72 ms with the tail (levels 4-5, one block
+// per visit) against 1.45 ms with the grid kernels -- one SM works through the 5049-point level
+// at tens of microseconds per visit where the grid launches spread each operation over all SMs.
+int tail_level(const mgp_solver* s) {
+    if (s->levels < 2 || s->lv[0].tune[MGP_TUNE_TAIL] != 1) return 0;
+    for (int l = 1; l < s->levels; l++) {
+        if (s->levels - l > kTailMaxLevels) continue;
+        size_t bytes = 0;
+        bool ok = true;
+        for (int m = l; m < s->levels; m++) {
+            bytes += tail_level_bytes(s, m);
+            ok = ok && !s->lv[m].gs_column && !s->lv[m].pair;
+        }
+        if (ok && bytes <= kTailMaxSmem) return l;
+    }
+    return 0;
+}
+
+template <typename T>
+int launch_tail(mgp_solver* s, int t0, bool fcycle, double omega, int64_t ns) {
+    TailArgs<T> a{};
+    static_assert(sizeof(TailArgs<T>) % sizeof(int) == 0, "the kernel copies its arguments as ints");
+    a.nl = s->levels - t0;
+    a.ns = (int)ns;
+    a.jacobi = s->desc.relaxation == MGP_JACOBI;
+    a.fw = s->desc.restriction == MGP_FULLWEIGHTING;
+    a.alt = s->gs_alternate;
+    int off = 0;
+    for (int m = 0; m < a.nl; m++) {
+        LevelState& L = s->lv[t0 + m];
+        TailLevel<T>& q = a.L[m];
+        q.G = L.G;
+        q.ub[0] = (T*)L.ubuf[0];
+        q.ub[1] = a.jacobi ? (T*)L.ubuf[1] : nullptr;
+        q.f = (T*)L.f;
+        q.r = (T*)L.r;
+        // constants as launch_stencil and bc_args form them (jacobi.h:41-44, neumann.h:117):
+        // the relaxation takes omega as a T, so it is rounded to T first
+        const T om = (T)omega;
+        q.two_h = (T)(2.0 * L.h);
+        q.hsq = (T)(L.h * L.h);
+        q.one_omega = (T)(1.0 - om);
+        q.omega_sixth = (T)(om / 6.0);
+        q.h = (T)L.h;
+        hsq_terms(q.hsq, q.inv_hsq, q.pow2);
+        const int n = L.G.nx * L.G.ny * L.G.nz;
+        q.so_u[0] = off;
+        off += n;
+        q.so_u[1] = a.jacobi ? off : q.so_u[0];
+        if (a.jacobi) off += n;
+        q.so_f = off;
+        off += n;
+        q.so_r = off;
+        off += n;
+        for (int f = 0; f < 6; f++) {
+            q.g[f] = (T*)L.face[f];
+            q.gn[f] = (int)(L.face_shape[f][0] * L.face_shape[f][1] * L.face_shape[f][2]);
+            q.neumann[f] = s->face_kind[f] == MGP_NEUMANN;
+            q.so_g[f] = off;
+            off += q.gn[f];
+        }
+        a.cur[m] = L.cur;
+    }
+    // The visit as a program (vcycle_t / fcycle_t's recursion), and the host state it leaves:
+    // each Jacobi sweep swaps the pair (a skipped first one included); red-black relaxations flip
+    // `alternate` 2*nsmooth times, which leaves it as it was.
+    a.nops = 0;
+    bool over = false;
+    auto emit = [&](int op, int m) {
+        if (a.nops >= kTailMaxOps) {
+            over = true;
+            return;
+        }
+        a.op[a.nops] = (unsigned char)op;
+        a.lv[a.nops] = (unsigned char)m;
+        a.nops++;
+    };
+    auto relax = [&](int m, bool skip) {
+        emit(skip ? TAIL_RELAX_SKIP1 : TAIL_RELAX, m);
+        if (a.jacobi) s->lv[t0 + m].cur ^= (int)(ns & 1);
+    };
+    const bool skip0 = s->lv[t0].first_done && ns > 0;
+    std::function<void(int, bool)> v = [&](int m, bool skip) {
+        relax(m, skip);
+        if (m >= a.nl - 1) return;
+        emit(TAIL_SETUP, m);
+        v(m + 1, false);
+        emit(TAIL_PROLONG, m);
+        relax(m, false);
+    };
+    std::function<void(int, bool)> f = [&](int m, bool skip) {
+        relax(m, skip);
+        emit(TAIL_SETUP, m);
+        if (m + 1 < a.nl - 1) f(m + 1, false);
+        v(m + 1, false);
+        emit(TAIL_PROLONG, m);
+    };
+    const uint64_t state_before = state_bits(s);
+    if (fcycle) f(0, skip0);
+    else v(0, skip0);
+    if (over) {
+        set_state_bits(s, state_before);
+        return fail(MGP_ERR_UNSUPPORTED, "coarse-level visit longer than %d operations", kTailMaxOps);
+    }
+    for (int m = 0; m < a.nl; m++) s->lv[t0 + m].first_done = false;
+    const size_t smem = (size_t)off * sizeof(T);
+    static bool attr_set[2][64] = {};
+    bool& set = attr_set[sizeof(T) == 8][s->device & 63];
+    if (!set) {
+        CK(cudaFuncSetAttribute(k_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTailMaxSmem));
+        set = true;
+    }
+    return launch_k(s, k_tail<T>, dim3(1), dim3(kTailThreads), smem, a);
+}
+
 // tail_norm: the caller's residual of level l with its max-norm, right after this cycle (the
 // solve loop's); the cycle's last relaxation may take it over and then sets *tail_done.
 template <typename T>
 int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns, unsigned long long* tail_norm = nullptr,
              bool* tail_done = nullptr) {
     // Vcycle<T> (include/vcycle.h:14-98)
+    if (!tail_norm && l >= 1 && l == tail_level(s)) return launch_tail<T>(s, l, false, omega, ns);
     const int tail = tail_norm ? RESID_NORM : RESID_NONE;
     if (l >= s->levels - 1) return relax_t<T>(s, l, omega, ns, false, tail, tail_norm, tail_done);
     bool rd = false;
@@ -977,6 +1109,7 @@ int fcycle_t(mgp_solver* s, int l, double omega, int64_t ns, unsigned long long*
              bool* tail_done = nullptr) {
     // Fcycle<T> (include/fcycle.h:13-97); the V-cycle of this level that follows relaxes it again
     if (tail_done) *tail_done = false;
+    if (!tail_norm && l >= 1 && l == tail_level(s)) return launch_tail<T>(s, l, true, omega, ns);
     bool rd = false;
     CKS(relax_t<T>(s, l, omega, ns, /*later=*/true, setup_residual_separate(s, l) ? RESID_STORE : RESID_NONE, nullptr,
                    &rd));
@@ -1950,6 +2083,9 @@ int autotune_search(mgp_solver* s, int cycle, int64_t ns, double omega, double* 
                 case MGP_TUNE_WAVE:
                     if (L.wave) cand = {1};
                     break;
+                case MGP_TUNE_TAIL:
+                    if (l == 0 && s->levels >= 2) cand = {1};
+                    break;
             }
             const int keep = L.tune[p];
             int chosen = keep;
@@ -1996,7 +2132,9 @@ int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value) {
     mgp_solver* t = s->inner ? s->inner : s;
     if (level < 0 || level >= t->levels) return fail(MGP_ERR_INVALID_ARG, "level %d out of range", level);
     if (param < 0 || param >= MGP_TUNE_PARAMS) return fail(MGP_ERR_INVALID_ARG, "unknown tuning parameter %d", param);
-    const int64_t hi = param == MGP_TUNE_SETUP_FORM ? 2 : param == MGP_TUNE_WAVE ? 1 : (int64_t)1 << 20;
+    const int64_t hi = param == MGP_TUNE_SETUP_FORM ? 2
+                       : (param == MGP_TUNE_WAVE || param == MGP_TUNE_TAIL) ? 1
+                                                                           : (int64_t)1 << 20;
     if (value < 0 || value > hi) return fail(MGP_ERR_INVALID_ARG, "tuning value %lld out of range", (long long)value);
     DeviceGuard guard(t->device);
     CK(cudaStreamSynchronize(t->stream));
