@@ -468,6 +468,8 @@ cudaError_t wave_prepare_level(mgp_solver* s, LevelState& L, int npair) {
     L.wave = false;
     L.pair = false;
     const Geom& G = L.G;
+    // the k-edge tensor maps carry one vector per row: TMA needs that to be 16 bytes
+    if (VecT<T>::V * sizeof(T) != 16) return cudaSuccess;
     if (s->desc.relaxation != MGP_JACOBI || !(s->desc.flags & MGP_FLAG_WAVE) || s->pool || !L.ubuf[1] ||
         s->levels > 31 || npair >= kPairMaxLevels || (long long)G.nx * G.ny * G.nz < kWaveMinPoints || G.nx < 3 ||
         G.ny < 3 || G.nz < 3 || !encode_tiled())

@@ -129,9 +129,15 @@ struct VecT<double> {
     static constexpr int V = 2;
     using type = double2;
 };
+// FP32 vector width: 4 (16-byte vectors) or, built with -DMGP_F32_VEC=2, 2 (8-byte vectors,
+// as many threads per plane as FP64).  Per-element arithmetic does not depend on it.
+#ifndef MGP_F32_VEC
+#define MGP_F32_VEC 4
+#endif
+static_assert(MGP_F32_VEC == 2 || MGP_F32_VEC == 4, "MGP_F32_VEC is 2 or 4");
 template <>
 struct VecT<float> {
-    static constexpr int V = 4;
+    static constexpr int V = MGP_F32_VEC;
     using type = float4;
 };
 
@@ -147,6 +153,11 @@ __device__ __forceinline__ void ldv(float (&d)[4], const float* p) {
     d[2] = x.z;
     d[3] = x.w;
 }
+__device__ __forceinline__ void ldv(float (&d)[2], const float* p) {
+    const float2 x = __ldg(reinterpret_cast<const float2*>(p));
+    d[0] = x.x;
+    d[1] = x.y;
+}
 // plain (coherent) vector loads for arrays the same kernel writes
 __device__ __forceinline__ void ldv_rw(double (&d)[2], const double* p) {
     const double2 x = *reinterpret_cast<const double2*>(p);
@@ -160,6 +171,14 @@ __device__ __forceinline__ void ldv_rw(float (&d)[4], const float* p) {
     d[2] = x.z;
     d[3] = x.w;
 }
+__device__ __forceinline__ void ldv_rw(float (&d)[2], const float* p) {
+    const float2 x = *reinterpret_cast<const float2*>(p);
+    d[0] = x.x;
+    d[1] = x.y;
+}
+__device__ __forceinline__ void stv(float* p, const float (&d)[2]) {
+    *reinterpret_cast<float2*>(p) = make_float2(d[0], d[1]);
+}
 __device__ __forceinline__ void stv(double* p, const double (&d)[2]) {
     *reinterpret_cast<double2*>(p) = make_double2(d[0], d[1]);
 }
@@ -167,11 +186,14 @@ __device__ __forceinline__ void stv(float* p, const float (&d)[4]) {
     *reinterpret_cast<float4*>(p) = make_float4(d[0], d[1], d[2], d[3]);
 }
 
-// Asynchronous 16-byte global->shared copies (cp.async, cached in L1 so that neighbouring
-// threads' in-plane reads of the same plane still hit L1).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+// Asynchronous global->shared copies (cp.async, cached in L1 so that neighbouring threads'
+// in-plane reads of the same plane still hit L1): one V-vector of T, 16 bytes (8 for 2-float
+// vectors), both addresses aligned to it.
+template <typename T>
+__device__ __forceinline__ void cp_async_vec(void* smem, const void* gmem) {
+    constexpr int B = VecT<T>::V * (int)sizeof(T);
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(B) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -190,9 +212,9 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
 template <typename T, int V>
 __device__ __forceinline__ void stage_f_or_r(T* slot, const T* f, const T* r, long long o, unsigned unr) {
     if (!unr) {
-        cp_async16(slot, f + o);
+        cp_async_vec<T>(slot, f + o);
     } else if (unr == (1u << V) - 1u) {
-        cp_async16(slot, r + o);
+        cp_async_vec<T>(slot, r + o);
     } else {
 #pragma unroll
         for (int e = 0; e < V; e++) cp_async_elem(slot + e, ((unr >> e) & 1u) ? r + o + e : f + o + e);
@@ -319,7 +341,7 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
             for (int st = 0; st < kStages; st++) {
                 const int p = i0 + st;
                 if (p < i1) {
-                    if (p + 1 < G.nx) cp_async16(su + st * SS, src + (long long)(p + 1) * G.sx + bjk);
+                    if (p + 1 < G.nx) cp_async_vec<T>(su + st * SS, src + (long long)(p + 1) * G.sx + bjk);
                     stage_f_or_r<T, V>(sf + st * SS, f, rr, (long long)p * G.sx + bjk, unr);
                 }
                 cp_async_commit();
@@ -348,8 +370,8 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                     {
                         const int q = i + kStages;
                         if (q < i1) {
-                            if (q + 1 < G.nx) cp_async16(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
-                            cp_async16(sf + slot * SS, f + (long long)q * G.sx + bjk);
+                            if (q + 1 < G.nx) cp_async_vec<T>(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
+                            cp_async_vec<T>(sf + slot * SS, f + (long long)q * G.sx + bjk);
                         }
                         cp_async_commit();
                     }
@@ -394,7 +416,7 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                 {  // refill this slot with plane i+kStages
                     const int q = i + kStages;
                     if (q < i1) {
-                        if (q + 1 < G.nx) cp_async16(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
+                        if (q + 1 < G.nx) cp_async_vec<T>(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
                         stage_f_or_r<T, V>(sf + slot * SS, f, rr, (long long)q * G.sx + bjk, unr);
                     }
                     cp_async_commit();
@@ -839,9 +861,13 @@ constexpr size_t rr_smem_bytes(int tkv, int rows) {
 }
 
 // 16-byte cp.async that bypasses L1 (the block reads the data from shared memory only)
-__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
+// One V-vector of T, not allocated in L1 where the size allows it (.cg exists for 16 bytes only)
+template <typename T>
+__device__ __forceinline__ void cp_async_vec_cg(void* smem, const void* gmem) {
+    constexpr int B = VecT<T>::V * (int)sizeof(T);
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    if (B == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(B) : "memory");
 }
 
 template <typename T>
@@ -934,12 +960,12 @@ __global__ void __launch_bounds__(384, 2) k_resid_restrict(RRArgs<T> a) {
         T* S = ring + st * STG;
         if (p <= pend) {
             const long long pp = (long long)p * Gf.sx;
-            if (ins) cp_async16_cg(S + s_own, u + pp + g_own);
-            if (c_hr) cp_async16_cg(S + s_hr, u + pp + g_hr);
+            if (ins) cp_async_vec_cg<T>(S + s_own, u + pp + g_own);
+            if (c_hr) cp_async_vec_cg<T>(S + s_hr, u + pp + g_hr);
             if (c_hc) cp_async_elem(S + s_hc, u + pp + g_hc);
             if (p <= ib) {
                 const bool inside = p >= Gf.x0 && p < Gf.x1;
-                if (ins) cp_async16_cg(S + s_f, (inside ? f : r) + pp + g_own);
+                if (ins) cp_async_vec_cg<T>(S + s_f, (inside ? f : r) + pp + g_own);
                 if (c_bd && inside) {
                     T* B = S + s_bd;
 #pragma unroll
@@ -1401,6 +1427,7 @@ __device__ __forceinline__ void ld_corr(double (&d)[2], const float* p) {
     d[1] = (double)x.y;
 }
 __device__ __forceinline__ void ld_corr(float (&d)[4], const float* p) { ldv(d, p); }
+__device__ __forceinline__ void ld_corr(float (&d)[2], const float* p) { ldv(d, p); }
 
 // Plane i (the tile's y index): one thread per k-vector of a row, u += (T) e where
 // (i, j, k) is inside the relaxation bounds.

@@ -157,10 +157,16 @@ __device__ __forceinline__ void sld(double (&d)[2], unsigned a) {
 __device__ __forceinline__ void sld(float (&d)[4], unsigned a) {
     asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n" : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3]) : "r"(a));
 }
+__device__ __forceinline__ void sld(float (&d)[2], unsigned a) {
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];\n" : "=f"(d[0]), "=f"(d[1]) : "r"(a));
+}
 __device__ __forceinline__ void sld1(double& v, unsigned a) { asm volatile("ld.shared.f64 %0, [%1];\n" : "=d"(v) : "r"(a)); }
 __device__ __forceinline__ void sld1(float& v, unsigned a) { asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(a)); }
 __device__ __forceinline__ void sst(unsigned a, const double (&d)[2]) {
     asm volatile("st.shared.v2.f64 [%0], {%1, %2};\n" ::"r"(a), "d"(d[0]), "d"(d[1]) : "memory");
+}
+__device__ __forceinline__ void sst(unsigned a, const float (&d)[2]) {
+    asm volatile("st.shared.v2.f32 [%0], {%1, %2};\n" ::"r"(a), "f"(d[0]), "f"(d[1]) : "memory");
 }
 __device__ __forceinline__ void sst(unsigned a, const float (&d)[4]) {
     asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(a), "f"(d[0]), "f"(d[1]), "f"(d[2]), "f"(d[3])
