@@ -803,7 +803,7 @@ def main():
         line["tuning"] = {"untuned_ms_per_iteration": tuning["untuned_ms"], "tuned_ms_per_iteration": tuning["tuned_ms"],
                           "search_s": tuning["search_s"],
                           "params_per_level": {"order": ["relax_planes", "resid_planes", "norm_planes", "setup_form",
-                                                         "setup_planes", "wave_off", "tail_off"],
+                                                         "setup_planes", "wave_off", "tail_on", "prolong_sweep_off"],
                                                "values": tuning["params"]}}
     if not args.no_extra:
         for key, fn in (("c1_fcycle_65", lambda: bench_c1(mgp, torch, local)),

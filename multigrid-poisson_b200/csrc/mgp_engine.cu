@@ -800,6 +800,43 @@ int prolong_t(mgp_solver* s, int l) {
     return launch_k(s, k_prolong<T, ADD>, grid, dim3(kThreads), 0, a);
 }
 
+// Prolongation + add and the first Jacobi sweep after it in one pass (k_prolong_sweep): Jacobi
+// levels >= 1, unless tuned off or relaxed by the wavefront passes, with nsmooth even and at
+// least 2.  Even: between the set-up that zeroed the coarse u and this prolongation the coarse
+// level is swept 2*nsmooth (V-cycle), nsmooth (coarsest level) or 3*nsmooth (F-cycle) times, so
+// with nsmooth even the prolongation reads the zeroed buffer, whose unrelaxed (Dirichlet)
+// points are +0 -- the condition under which the kernel may leave u' unstored.  With nsmooth
+// odd it reads the other buffer, whose Dirichlet points hold whatever they held.
+bool prolong_sweep_fused(const mgp_solver* s, int l, int64_t ns) {
+    const LevelState& L = s->lv[l];
+    return s->desc.relaxation == MGP_JACOBI && l >= 1 && ns >= 2 && (ns & 1) == 0 && !L.wave && !L.first_done &&
+           L.tune[MGP_TUNE_PROLONG_SWEEP] != 1;
+}
+
+template <typename T>
+int prolong_sweep_t(mgp_solver* s, int l, double omega) {
+    LevelState& F = s->lv[l];
+    LevelState& C = s->lv[l + 1];
+    ProlongSweepArgs<T> a;
+    a.uc = (const T*)u_ptr(s, l + 1);
+    a.Gc = C.G;
+    a.u = (T*)u_ptr(s, l);
+    a.dst = (T*)uprev_ptr(s, l);
+    a.f = (const T*)F.f;
+    a.r = (T*)F.r;
+    a.Gf = F.G;
+    a.F = faces_of<T>(s, l);
+    const T om = (T)omega;  // the relaxation takes omega as a T (jacobi.h:41-44)
+    a.two_h = (T)(2.0 * F.h);
+    a.hsq = (T)(F.h * F.h);
+    a.one_omega = (T)(1.0 - om);
+    a.omega_sixth = (T)(om / 6.0);
+    const dim3 grid((F.G.ny * F.G.nz + kThreads - 1) / kThreads, F.G.nx);
+    CKS(launch_k(s, k_prolong_sweep<T>, grid, dim3(kThreads), 0, a));
+    F.cur ^= 1;  // the sweep's swap_u: u is now the other buffer
+    return MGP_OK;
+}
+
 template <typename T>
 int add_t(mgp_solver* s, int l) {
     LevelState& L = s->lv[l];
@@ -1101,6 +1138,10 @@ int vcycle_t(mgp_solver* s, int l, double omega, int64_t ns, unsigned long long*
                    &rd));
     CKS(coarse_setup_t<T>(s, l, omega, ns, rd));
     CKS(vcycle_t<T>(s, l + 1, omega, ns));
+    if (!tail_norm && prolong_sweep_fused(s, l, ns)) {
+        CKS(prolong_sweep_t<T>(s, l, omega));
+        return relax_t<T>(s, l, omega, ns - 1, false, tail, tail_norm, tail_done);
+    }
     CKS((prolong_t<T, true>(s, l)));
     CKS(relax_t<T>(s, l, omega, ns, false, tail, tail_norm, tail_done));
     return MGP_OK;
@@ -2088,6 +2129,9 @@ int autotune_search(mgp_solver* s, int cycle, int64_t ns, double omega, double* 
                 case MGP_TUNE_TAIL:
                     if (l == 0 && s->levels >= 2) cand = {1};
                     break;
+                case MGP_TUNE_PROLONG_SWEEP:
+                    if (coarser && l >= 1 && s->desc.relaxation == MGP_JACOBI && ns >= 2 && !(ns & 1)) cand = {1};
+                    break;
             }
             const int keep = L.tune[p];
             int chosen = keep;
@@ -2135,8 +2179,9 @@ int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value) {
     if (level < 0 || level >= t->levels) return fail(MGP_ERR_INVALID_ARG, "level %d out of range", level);
     if (param < 0 || param >= MGP_TUNE_PARAMS) return fail(MGP_ERR_INVALID_ARG, "unknown tuning parameter %d", param);
     const int64_t hi = param == MGP_TUNE_SETUP_FORM ? 2
-                       : (param == MGP_TUNE_WAVE || param == MGP_TUNE_TAIL) ? 1
-                                                                           : (int64_t)1 << 20;
+                       : (param == MGP_TUNE_WAVE || param == MGP_TUNE_TAIL || param == MGP_TUNE_PROLONG_SWEEP)
+                           ? 1
+                           : (int64_t)1 << 20;
     if (value < 0 || value > hi) return fail(MGP_ERR_INVALID_ARG, "tuning value %lld out of range", (long long)value);
     DeviceGuard guard(t->device);
     CK(cudaStreamSynchronize(t->stream));

@@ -1234,6 +1234,80 @@ __device__ __forceinline__ void prolong_tile(const ProlongArgs<T>& a, const int 
         }
 }
 
+// ---- prolongation + add fused with the first Jacobi sweep after it (levels >= 1, nsmooth even) --
+// u' = u + P u_c, then one sweep of u' into the other buffer, in one pass: every thread forms
+// u' at its point and at the six neighbours from u and the coarse values (the arithmetic of
+// prolong_tile) and sweeps (jacobi.h:59-61), writing the other buffer at relaxed points.  u' is
+// not stored at relaxed points: the second sweep of the relaxation overwrites them before
+// anything reads them.  At unrelaxed (Dirichlet) points P u_c is exactly +0 -- with nsmooth
+// even the coarse u read here is the buffer the set-up zeroed, whose Dirichlet points stay +0
+// (prolong_sweep_fused in mgp_engine.cu) -- so u there becomes u + 0 in place (a reader that
+// sees the old or the new value forms the same u + 0) and r takes P u_c, as prolong_tile
+// leaves it.
+template <typename T>
+struct ProlongSweepArgs {
+    const T* uc;
+    Geom Gc;
+    T* u;        // current u (read; written at unrelaxed points)
+    T* dst;      // the other buffer: the sweep's result at relaxed points
+    const T* f;
+    T* r;
+    Geom Gf;
+    Faces<T> F;
+    T two_h, hsq, one_omega, omega_sixth;
+};
+
+template <typename T>
+__device__ __forceinline__ T prolong_value(const T* __restrict__ uc, const Geom& C, int i, int j, int k) {
+    auto Cv = [&](int x, int y, int z) -> T {
+        return (x < C.nx && y < C.ny && z < C.nz) ? ldg(uc + x * C.sx + y * C.sy + z) : T(0);
+    };
+    const int ic = i >> 1, jc = j >> 1, kc = k >> 1;
+    T yv[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        T x0 = Cv(ic, jc, kc + q), x1 = Cv(ic, jc + 1, kc + q);
+        if (i & 1) {
+            x0 = half_sum(x0, Cv(ic + 1, jc, kc + q));
+            x1 = half_sum(x1, Cv(ic + 1, jc + 1, kc + q));
+        }
+        yv[q] = (j & 1) ? half_sum(x0, x1) : x0;
+    }
+    return (k & 1) ? half_sum(yv[0], yv[1]) : yv[0];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_sweep(ProlongSweepArgs<T> a) {
+    pdl_begin();
+    const Geom& G = a.Gf;
+    const int t = blockIdx.x * 256 + (int)threadIdx.x;
+    if (t >= G.ny * G.nz) return;
+    const int i = blockIdx.y, j = t / G.nz, k = t - (t / G.nz) * G.nz;
+    const long long p = (long long)i * G.sx + (long long)j * G.sy + k;
+    const bool relaxed = i >= G.x0 && i < G.x1 && j >= G.y0 && j < G.y1 && k >= G.z0 && k < G.z1;
+    if (!relaxed) {
+        const T e = prolong_value(a.uc, a.Gc, i, j, k);
+        a.u[p] = a.u[p] + e;
+        a.r[p] = e;
+        return;
+    }
+    // u' at a point of the level
+    auto U = [&](int x, int y, int z) -> T {
+        const long long q = (long long)x * G.sx + (long long)y * G.sy + z;
+        return a.u[q] + prolong_value(a.uc, a.Gc, x, y, z);
+    };
+    const T two_h = a.two_h, m2h = -a.two_h;
+    const T uc0 = U(i, j, k);
+    const T vm = i > 0 ? U(i - 1, j, k) : m2h * ldg(a.F.g[F_WEST] + (long long)j * G.nz + k) + U(1, j, k);
+    const T vp = i < G.nx - 1 ? U(i + 1, j, k) : two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + k) + U(G.nx - 2, j, k);
+    const T ym = j > 0 ? U(i, j - 1, k) : m2h * ldg(a.F.g[F_SOUTH] + (long long)i * G.nz + k) + U(i, 1, k);
+    const T yp = j < G.ny - 1 ? U(i, j + 1, k) : two_h * ldg(a.F.g[F_NORTH] + (long long)i * G.nz + k) + U(i, G.ny - 2, k);
+    const T zm = k > 0 ? U(i, j, k - 1) : m2h * ldg(a.F.g[F_BOTTOM] + (long long)i * G.ny + j) + U(i, j, 1);
+    const T zp = k < G.nz - 1 ? U(i, j, k + 1) : two_h * ldg(a.F.g[F_TOP] + (long long)i * G.ny + j) + U(i, j, G.nz - 2);
+    const T sum = vm + vp + ym + yp + zm + zp;
+    a.dst[p] = a.one_omega * uc0 + a.omega_sixth * (sum - a.hsq * ldg(a.f + p));
+}
+
 template <typename T, bool ADD>
 __global__ void __launch_bounds__(256) k_prolong(ProlongArgs<T> a) {
     pdl_begin();

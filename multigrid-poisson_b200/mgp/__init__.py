@@ -42,8 +42,9 @@ FLAG_REFINE_F64 = 32
 FLAG_WAVE = 256
 SOLVE_VERBOSE, SOLVE_PRINT_CYCLE_TIME = 1, 2
 # launch-shape tuning parameters (mgp_set_tuning / mgp_autotune)
-TUNE_RELAX_PLANES, TUNE_RESID_PLANES, TUNE_NORM_PLANES, TUNE_SETUP_FORM, TUNE_SETUP_PLANES, TUNE_WAVE, TUNE_TAIL = range(7)
-TUNE_PARAMS = 7
+(TUNE_RELAX_PLANES, TUNE_RESID_PLANES, TUNE_NORM_PLANES, TUNE_SETUP_FORM, TUNE_SETUP_PLANES, TUNE_WAVE, TUNE_TAIL,
+ TUNE_PROLONG_SWEEP) = range(8)
+TUNE_PARAMS = 8
 AUTOTUNE_FORCE = 1
 
 _RESTRICTIONS = {"Injection": INJECTION, "injection": INJECTION, "inj": INJECTION,
