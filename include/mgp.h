@@ -244,8 +244,9 @@ int mgp_norm(mgp_solver* s, int field, int level, double* out);
 #define MGP_TUNE_TAIL 6         /* level 0 only: 1 runs each cycle visit of the coarsest levels that fit in one
                                    CTA's shared memory as one launch of one block; 0 (built-in) keeps the
                                    grid kernels, which are faster on B200 for the 513x257x129 hierarchy */
-#define MGP_TUNE_PROLONG_SWEEP 7 /* 0 built-in (Jacobi levels >= 1 with nsmooth >= 2 fuse the prolongation +
-                                    add with the first sweep after it), 1 separate passes */
+#define MGP_TUNE_PROLONG_SWEEP 7 /* prolongation + add fused with the first Jacobi sweep after it (levels >= 1,
+                                    nsmooth even): 0 built-in (levels of at most 2^16 points), 1 separate
+                                    passes, 2 fused */
 #define MGP_TUNE_PARAMS 8
 int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value);
 int mgp_get_tuning(mgp_solver* s, int level, int param, int64_t* value);

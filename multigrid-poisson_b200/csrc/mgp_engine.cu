@@ -807,10 +807,18 @@ int prolong_t(mgp_solver* s, int l) {
 // with nsmooth even the prolongation reads the zeroed buffer, whose unrelaxed (Dirichlet)
 // points are +0 -- the condition under which the kernel may leave u' unstored.  With nsmooth
 // odd it reads the other buffer, whose Dirichlet points hold whatever they held.
+// Built in only on levels of at most 2^16 points (MGP_TUNE_PROLONG_SWEEP = 2 forces it): forming
+// u' at seven points per thread makes larger levels instruction-bound -- on B200 the 513x257x129
+// F-cycle iteration took 1.585 ms fused on levels 1-4 against 1.453 ms separate, and the
+// autotuner keeps the separate passes on its 2.15M- and 277K-point levels.
+constexpr long long kProlongSweepMaxPoints = 1ll << 16;
 bool prolong_sweep_fused(const mgp_solver* s, int l, int64_t ns) {
     const LevelState& L = s->lv[l];
-    return s->desc.relaxation == MGP_JACOBI && l >= 1 && ns >= 2 && (ns & 1) == 0 && !L.wave && !L.first_done &&
-           L.tune[MGP_TUNE_PROLONG_SWEEP] != 1;
+    const int t = L.tune[MGP_TUNE_PROLONG_SWEEP];
+    if (!(s->desc.relaxation == MGP_JACOBI && l >= 1 && ns >= 2 && (ns & 1) == 0 && !L.wave && !L.first_done) ||
+        t == 1)
+        return false;
+    return t == 2 || (long long)L.G.nx * L.G.ny * L.G.nz <= kProlongSweepMaxPoints;
 }
 
 template <typename T>
@@ -2130,7 +2138,7 @@ int autotune_search(mgp_solver* s, int cycle, int64_t ns, double omega, double* 
                     if (l == 0 && s->levels >= 2) cand = {1};
                     break;
                 case MGP_TUNE_PROLONG_SWEEP:
-                    if (coarser && l >= 1 && s->desc.relaxation == MGP_JACOBI && ns >= 2 && !(ns & 1)) cand = {1};
+                    if (coarser && l >= 1 && s->desc.relaxation == MGP_JACOBI && ns >= 2 && !(ns & 1)) cand = {1, 2};
                     break;
             }
             const int keep = L.tune[p];
@@ -2179,9 +2187,9 @@ int mgp_set_tuning(mgp_solver* s, int level, int param, int64_t value) {
     if (level < 0 || level >= t->levels) return fail(MGP_ERR_INVALID_ARG, "level %d out of range", level);
     if (param < 0 || param >= MGP_TUNE_PARAMS) return fail(MGP_ERR_INVALID_ARG, "unknown tuning parameter %d", param);
     const int64_t hi = param == MGP_TUNE_SETUP_FORM ? 2
-                       : (param == MGP_TUNE_WAVE || param == MGP_TUNE_TAIL || param == MGP_TUNE_PROLONG_SWEEP)
-                           ? 1
-                           : (int64_t)1 << 20;
+                       : (param == MGP_TUNE_WAVE || param == MGP_TUNE_TAIL) ? 1
+                       : param == MGP_TUNE_PROLONG_SWEEP ? 2
+                                                           : (int64_t)1 << 20;
     if (value < 0 || value > hi) return fail(MGP_ERR_INVALID_ARG, "tuning value %lld out of range", (long long)value);
     DeviceGuard guard(t->device);
     CK(cudaStreamSynchronize(t->stream));

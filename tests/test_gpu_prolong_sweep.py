@@ -31,10 +31,10 @@ def test_fused_matches_separate(mgp_mod, gpu_ready, ci, dtype, cycle, ns):
     dt = mgp_mod.F64 if dtype == "f64" else mgp_mod.F32
     npdt = np.float64 if dtype == "f64" else np.float32
     engines = []
-    for off in (0, 1):
+    for mode in (2, 1):  # fused on every eligible level, separate passes
         e = make_engine(mgp_mod, cfg, dtype=dt)
         for l in range(levels):
-            e.set_tuning(l, mgp_mod.TUNE_PROLONG_SWEEP, off)
+            e.set_tuning(l, mgp_mod.TUNE_PROLONG_SWEEP, mode)
             for name in ("u", "uprev", "f", "r"):
                 e.upload(name, o.field(name, l).astype(npdt), l)
             for fc in range(6):
@@ -61,6 +61,8 @@ def test_fused_cycles_match_oracle(mgp_mod, gpu_ready, ci, cycle):
     o = make_oracle(cfg)
     randomize(o, 140 + ci)
     e = make_engine(mgp_mod, cfg)
+    for l in range(levels):
+        e.set_tuning(l, mgp_mod.TUNE_PROLONG_SWEEP, 2)
     push(o, e)
     om = o.default_omega()
     for ns in (3, 2):

@@ -113,7 +113,7 @@ def test_tuning_rejects_bad_arguments(mgp_mod, gpu_ready):
     cfg = SOLVE_CFGS[0]
     e = make_engine(mgp_mod, cfg)
     for level, param, value in ((-1, 0, 1), (4, 0, 1), (0, mgp_mod.TUNE_PARAMS, 1), (0, -1, 1), (0, 0, -1), (0, 3, 3),
-                                (0, 5, 2), (0, 6, 2), (1, 7, 2)):
+                                (0, 5, 2), (0, 6, 2), (1, 7, 3)):
         with pytest.raises(mgp_mod.MgpError) as ei:
             e.set_tuning(level, param, value)
         assert ei.value.status == mgp_mod.ERR_INVALID_ARG
