@@ -512,6 +512,8 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
 }
 
 template <typename T, int OP, bool NORM>
+// (more resident blocks requested through __launch_bounds__ measured slower on B200: 5 per SM
+// at 48 registers 85 us per level-0 sweep, 6 at 40 registers 132 us, against 80-82 us at 64)
 __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
     pdl_begin();
     stencil_tile<T, OP, NORM>(a, blockIdx.x, blockIdx.y);
