@@ -561,6 +561,41 @@ __device__ __forceinline__ T fw_point(const T* in, const View& vi, int i, int j,
     return fw_sum<T>(A, im, ii, ip, jm, jj, jp, km, kk, kp);
 }
 
+// fw_point for a thread of a warp whose lanes hold consecutive coarse points t of one coarse
+// plane (t = j*n[2] + k).  Each fine row of the 3x3 neighbourhood is read as the aligned pair
+// (2k, 2k+1) in one 2-element load; the value at 2k-1 is the second element of lane-1's pair
+// when that lane holds (j, k-1), else (first lane of the warp, or k = 0) a scalar load or the
+// clamped centre.  Same values and the same sums as fw_point.  Every lane of the warp must
+// call it (lanes without a point with any point of the plane); the fine rows hold an odd
+// number of points at an even pitch, so 2k+1 lies inside the row's pitch.
+template <typename T>
+__device__ __forceinline__ T fw_point_pairs(const T* in, const View& vi, int i, int j, int k) {
+    const int ii = min(vi.n[0] - 1, 2 * i), jj = min(vi.n[1] - 1, 2 * j), kk = 2 * k;
+    const int im = max(0, ii - 1), ip = min(vi.n[0] - 1, ii + 1);
+    const int jm = max(0, jj - 1), jp = min(vi.n[1] - 1, jj + 1);
+    const bool from_lane = (threadIdx.x & 31) != 0 && k > 0;
+    const bool clamp_p = kk + 1 > vi.n[2] - 1;  // kp = kk
+    const int X[3] = {im, ii, ip}, Y[3] = {jm, jj, jp};
+    double vm[3][3], v0[3][3], vp[3][3];
+#pragma unroll
+    for (int x = 0; x < 3; x++)
+#pragma unroll
+        for (int y = 0; y < 3; y++) {
+            const T* row = in + X[x] * vi.s0 + Y[y] * vi.s1;
+            T pr[2];
+            ldv(pr, row + kk);
+            const T prev = __shfl_up_sync(0xffffffffu, pr[1], 1);
+            v0[x][y] = (double)pr[0];
+            vp[x][y] = (double)(clamp_p ? pr[0] : pr[1]);
+            T m = pr[0];  // k = 0: km = kk
+            if (k > 0) m = from_lane ? prev : ldg(row + kk - 1);
+            vm[x][y] = (double)m;
+        }
+    // fw_sum over the positions (0, 1, 2) = (m, centre, p) of the neighbourhood along each axis
+    auto A = [&](int x, int y, int z) -> double { return z == 0 ? vm[x][y] : (z == 1 ? v0[x][y] : vp[x][y]); };
+    return fw_sum<T>(A, 0, 1, 2, 0, 1, 2, 0, 1, 2);
+}
+
 template <typename T>
 struct RestrictArgs;
 
@@ -641,14 +676,17 @@ __device__ __forceinline__ void coarse_u_write(const FirstSweep<T>& w, T* zero_u
 template <typename T, bool FS = false>
 __device__ __forceinline__ void restrict_tile(const RestrictArgs<T>& a, const int bx, const int i) {
     const View vo = a.vo;
+    const int n = vo.n[1] * vo.n[2];
     const int t = bx * 256 + (int)threadIdx.x;
-    if (t >= vo.n[1] * vo.n[2]) return;
-    const int j = t / vo.n[2];
-    const int k = t - j * vo.n[2];
+    if (bx * 256 + (int)(threadIdx.x & ~31u) >= n) return;  // whole warps past the plane
+    // lanes past the plane compute the last point (fw_point_pairs needs every lane of a warp)
+    const int tc = min(t, n - 1);
+    const int j = tc / vo.n[2];
+    const int k = tc - j * vo.n[2];
+    const T v = a.fw ? fw_point_pairs(a.in, a.vi, i, j, k)
+                     : ldg(a.in + (2 * i) * a.vi.s0 + (2 * j) * a.vi.s1 + 2 * k);  // injection.h:63
+    if (t >= n) return;
     const long long o = i * vo.s0 + j * vo.s1 + k;
-    T v;
-    if (a.fw) v = fw_point(a.in, a.vi, i, j, k);
-    else v = ldg(a.in + (2 * i) * a.vi.s0 + (2 * j) * a.vi.s1 + 2 * k);  // injection.h:63
     a.out[o] = v;
     if (FS) {
         auto g = [&](int fc, int fi, int fj, int fk) -> T {  // coarse faces restricted before this launch
