@@ -640,6 +640,10 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
     dim3 grid(bx, chunks);
+    if (OP != OP_GS_COLUMN && a.ichunk == 1) {  // one plane per block: the one-round-trip form
+        if (OP == OP_RESIDUAL && norm) return launch_k(s, k_stencil<T, OP, true, true>, grid, dim3(kThreads), 0, a);
+        return launch_k(s, k_stencil<T, OP, false, true>, grid, dim3(kThreads), 0, a);
+    }
     if (OP == OP_RESIDUAL && norm) return launch_k(s, k_stencil<T, OP, true>, grid, dim3(kThreads), 0, a);
     return launch_k(s, k_stencil<T, OP, false>, grid, dim3(kThreads), 0, a);
 }

@@ -251,13 +251,37 @@ __device__ __forceinline__ void plane_vector(int t, int ny, int nv, int& j, int&
     }
 }
 
+// The stencil at an interior vector (every neighbour a point of the level, every point
+// relaxed): the relaxation or the residual of its V points from u(i-1), u(i), u(i+1), f, rows
+// j-1 and j+1 and the k-1 / k+V values.  base: red-black colour of element 0.
+template <typename T, int OP, bool NORM, int V>
+__device__ __forceinline__ void interior_vector(const StencilArgs<T>& a, const T (&vm)[V], const T (&vc)[V],
+                                                const T (&vp)[V], const T (&fc)[V], const T (&ym)[V],
+                                                const T (&yp)[V], T left, T right, int base, T (&cur)[V],
+                                                unsigned long long& mx) {
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const T below = e > 0 ? vc[e - 1] : left;
+        const T above = e < V - 1 ? vc[e + 1] : right;
+        const T sum = vm[e] + vp[e] + ym[e] + yp[e] + below + above;
+        if (OP == OP_RESIDUAL) {
+            const T r = residual_pt(fc[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
+            cur[e] = r;
+            if (NORM) mx = max(mx, abs_bits(r));
+        } else {
+            const T v = a.one_omega * vc[e] + a.omega_sixth * (sum - a.hsq * fc[e]);
+            cur[e] = (OP == OP_GS && ((base + e) & 1) != a.colour) ? vc[e] : v;
+        }
+    }
+}
+
 // One thread owns a V-vector of k points of one (j) row and marches i over a chunk of
 // planes with u(i-1), u(i), u(i+1) in registers.  The next kStages planes of u and f are
 // staged by cp.async into the thread's own shared-memory slots, so each thread keeps
 // 2*kStages*16 bytes in flight without a block barrier.  For small levels the chunk is a
 // single plane (one point-vector per thread).  NORM adds the max-norm of the residual
 // over the whole shape.
-template <typename T, int OP, bool NORM>
+template <typename T, int OP, bool NORM, bool ONE = false>
 __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int bx, const int by) {
     constexpr int V = VecT<T>::V;
     __shared__ __align__(16) T stage_u[kStages][256 * V];
@@ -336,9 +360,14 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
             const unsigned unr = 0u;  // elements that would stage r in place of f (none)
             const T* rr = a.dst;
             constexpr int SS = 256 * V;  // stage stride
-            // stage s holds u(i0+s+1) and f(i0+s)
+            // stage s holds u(i0+s+1) and f(i0+s).  ONE (launched with one plane per block, on
+            // small levels): nothing is staged; u(i+1) and f are loaded with the in-plane
+            // neighbours, so every load of the thread is in flight at once -- one round trip to
+            // memory instead of two (the staged march waits for its copies before it issues the
+            // in-plane loads).
 #pragma unroll
             for (int st = 0; st < kStages; st++) {
+                if (ONE) break;
                 const int p = i0 + st;
                 if (p < i1) {
                     if (p + 1 < G.nx) cp_async_vec<T>(su + st * SS, src + (long long)(p + 1) * G.sx + bjk);
@@ -364,10 +393,13 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                 const int slot = (i - i0) % kStages;
                 if (fast && i >= 1 && i + 1 < G.nx) {
                     // the condition-free body: every neighbour is a point of the level
-                    cp_async_wait<kStages - 1>();
-                    lds_v(vp, su + slot * SS);
-                    lds_v(fc, sf + slot * SS);
-                    {
+                    if (ONE) {
+                        ldv(vp, src + p + G.sx);
+                        ldv(fc, f + p);
+                    } else {
+                        cp_async_wait<kStages - 1>();
+                        lds_v(vp, su + slot * SS);
+                        lds_v(fc, sf + slot * SS);
                         const int q = i + kStages;
                         if (q < i1) {
                             if (q + 1 < G.nx) cp_async_vec<T>(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
@@ -379,21 +411,8 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                     ldv(ym, src + p - G.sy);
                     ldv(yp, src + p + G.sy);
                     const T left = ldg(src + p - 1), right = ldg(src + p + V);
-                    const int base = i + j + kb + G.poff;  // red-black colour of element 0
-#pragma unroll
-                    for (int e = 0; e < V; e++) {
-                        const T below = e > 0 ? vc[e - 1] : left;
-                        const T above = e < V - 1 ? vc[e + 1] : right;
-                        const T sum = vm[e] + vp[e] + ym[e] + yp[e] + below + above;
-                        if (OP == OP_RESIDUAL) {
-                            const T r = residual_pt(fc[e], sum, vc[e], a.hsq, a.inv_hsq, a.hsq_pow2);
-                            cur[e] = r;
-                            if (NORM) mx = max(mx, abs_bits(r));
-                        } else {
-                            const T v = a.one_omega * vc[e] + a.omega_sixth * (sum - a.hsq * fc[e]);
-                            cur[e] = (OP == OP_GS && ((base + e) & 1) != a.colour) ? vc[e] : v;
-                        }
-                    }
+                    interior_vector<T, OP, NORM, V>(a, vm, vc, vp, fc, ym, yp, left, right, i + j + kb + G.poff, cur,
+                                                    mx);
                     stv(a.dst + p, cur);
 #pragma unroll
                     for (int e = 0; e < V; e++) {
@@ -403,17 +422,19 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
                     }
                     continue;
                 }
-                cp_async_wait<kStages - 1>();
+                if (!ONE) cp_async_wait<kStages - 1>();
                 if (i + 1 < G.nx) {
-                    lds_v(vp, su + slot * SS);
+                    if (ONE) ldv(vp, src + p + G.sx);
+                    else lds_v(vp, su + slot * SS);
                 } else {  // east ghost  2h*gE + u(nx-2), from before this sweep
 #pragma unroll
                     for (int e = 0; e < V; e++)
                         vp[e] = ((ins >> e) & 1u) ? two_h * ldg(a.F.g[F_EAST] + (long long)j * G.nz + kb + e) + vmo[e]
                                                   : T(0);
                 }
-                lds_v(fc, sf + slot * SS);
-                {  // refill this slot with plane i+kStages
+                if (ONE) ldv(fc, f + p);  // stage_f_or_r with no r lanes
+                else lds_v(fc, sf + slot * SS);
+                if (!ONE) {  // refill this slot with plane i+kStages
                     const int q = i + kStages;
                     if (q < i1) {
                         if (q + 1 < G.nx) cp_async_vec<T>(su + slot * SS, src + (long long)(q + 1) * G.sx + bjk);
@@ -511,12 +532,12 @@ __device__ __forceinline__ void stencil_tile(const StencilArgs<T>& a, const int 
     if (NORM) block_max_to(mx, a.norm);
 }
 
-template <typename T, int OP, bool NORM>
+template <typename T, int OP, bool NORM, bool ONE = false>
 // (more resident blocks requested through __launch_bounds__ measured slower on B200: 5 per SM
 // at 48 registers 85 us per level-0 sweep, 6 at 40 registers 132 us, against 80-82 us at 64)
 __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
     pdl_begin();
-    stencil_tile<T, OP, NORM>(a, blockIdx.x, blockIdx.y);
+    stencil_tile<T, OP, NORM, ONE>(a, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------------------------------
