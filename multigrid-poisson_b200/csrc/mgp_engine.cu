@@ -16,6 +16,7 @@
 #include <cstring>
 #include <fstream>
 #include <functional>
+#include <type_traits>
 #include <iomanip>
 #include <iostream>
 #include <cstdlib>
@@ -632,7 +633,9 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
             chunks = (L.G.nx + planes - 1) / planes;
         } else {
             const int cap = sm_count(s->device) *
-                            (nrm ? resident_blocks(k_stencil<T, OP, true>) : resident_blocks(k_stencil<T, OP, false>));
+                            (nrm ? (std::is_same<T, double>::value ? resident_blocks(k_residual_norm64<false>)
+                                                                    : resident_blocks(k_stencil<T, OP, true>))
+                                 : resident_blocks(k_stencil<T, OP, false>));
             chunks = march_chunks(bx, L.G.nx, cap);
             chunks = short_march_chunks<T>(L.G, bx, cap, chunks);
         }
@@ -640,6 +643,12 @@ int launch_stencil(mgp_solver* s, int l, const void* src, void* dst, T omega, in
     a.ichunk = (L.G.nx + chunks - 1) / chunks;
     chunks = (L.G.nx + a.ichunk - 1) / a.ichunk;
     dim3 grid(bx, chunks);
+    if constexpr (std::is_same<T, double>::value && OP == OP_RESIDUAL) {
+        if (norm) {
+            if (a.ichunk == 1) return launch_k(s, k_residual_norm64<true>, grid, dim3(kThreads), 0, a);
+            return launch_k(s, k_residual_norm64<false>, grid, dim3(kThreads), 0, a);
+        }
+    }
     if (OP != OP_GS_COLUMN && a.ichunk == 1) {  // one plane per block: the one-round-trip form
         if (OP == OP_RESIDUAL && norm) return launch_k(s, k_stencil<T, OP, true, true>, grid, dim3(kThreads), 0, a);
         return launch_k(s, k_stencil<T, OP, false, true>, grid, dim3(kThreads), 0, a);

@@ -540,6 +540,14 @@ __global__ void __launch_bounds__(256) k_stencil(StencilArgs<T> a) {
     stencil_tile<T, OP, NORM, ONE>(a, blockIdx.x, blockIdx.y);
 }
 
+// The FP64 residual with its max-norm (the solve loop's): held to 64 registers, 4 blocks per SM
+// (unbounded it takes 74 and 3 blocks).
+template <bool ONE>
+__global__ void __launch_bounds__(256, 4) k_residual_norm64(StencilArgs<double> a) {
+    pdl_begin();
+    stencil_tile<double, OP_RESIDUAL, true, ONE>(a, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------------------------------
 // Restriction r_l -> f_{l+1} over the coarse shape, with u_{l+1} = 0 fused in
 // (include/vcycle.h:43-50).  Works on any pair of (shape, strides) views, so the same code
