@@ -199,6 +199,13 @@ int mgp_set_iteration_limits(mgp_solver* s, int64_t maxiter, int64_t miniter, do
  * half-sweeps (Jacobi ping-pong / red-black SOR) with the Neumann ghost values formed in
  * the kernel. */
 int mgp_relax(mgp_solver* s, int level, double omega, int64_t nsmooth);
+/* One red-black half-sweep of `level` over the points of colour `colour` (0 or 1: the parity
+ * of the reference's padded linear index on this solver's level, the colour
+ * GaussSeidel::relaxation_kernel updates in one call, include/gaussseidel.h:28-94), in place,
+ * with the solver's alternate flag neither read nor changed.  For callers that order the
+ * colours themselves: a domain split into slabs exchanges its halo planes between the two
+ * half-sweeps.  UNSUPPORTED for Jacobi solvers. */
+int mgp_relax_colour(mgp_solver* s, int level, double omega, int colour);
 /* Failure detection of the wavefront passes (MGP_FLAG_WAVE): bound on the polls of a wait for a
  * plane copy (0 = the default, 2^22).  A wait that runs out marks the pass failed; the pass
  * still lets every copy it issued land before it exits, and the next norm read-back (the solve

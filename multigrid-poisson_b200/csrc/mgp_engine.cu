@@ -715,6 +715,16 @@ int relax_t(mgp_solver* s, int l, double omega, int64_t nsmooth, bool later = fa
     return MGP_OK;
 }
 
+// One red-black half-sweep of a given colour (mgp_relax_colour); the alternate flag stays.
+template <typename T>
+int relax_colour_t(mgp_solver* s, int l, double omega, int colour) {
+    LevelState& L = s->lv[l];
+    L.first_done = false;
+    void* u = u_ptr(s, l);
+    if (L.gs_column) return launch_stencil<T, OP_GS_COLUMN>(s, l, u, u, (T)omega, colour, nullptr);
+    return launch_stencil<T, OP_GS>(s, l, u, u, (T)omega, colour, nullptr);
+}
+
 template <typename T>
 int residual_t(mgp_solver* s, int l, unsigned long long* norm) {
     LevelState& L = s->lv[l];
@@ -1877,6 +1887,15 @@ int mgp_relax(mgp_solver* s, int l, double omega, int64_t nsmooth) {
     DeviceGuard guard(s->device);
     if (omega < 0) omega = s->desc.relaxation == MGP_JACOBI ? 6.0 / 7.0 : 8.0 / 9.0;
     return DISPATCH(s, (relax_t<T>(s, l, omega, nsmooth)));
+}
+int mgp_relax_colour(mgp_solver* s, int l, double omega, int colour) {
+    CKS(validate_level(s, l));
+    if (s->desc.relaxation != MGP_GAUSSSEIDEL)
+        return fail(MGP_ERR_UNSUPPORTED, "mgp_relax_colour: the solver relaxes with Jacobi");
+    if (colour != 0 && colour != 1) return fail(MGP_ERR_INVALID_ARG, "colour must be 0 or 1");
+    DeviceGuard guard(s->device);
+    if (omega < 0) omega = 8.0 / 9.0;
+    return DISPATCH(s, (relax_colour_t<T>(s, l, omega, colour)));
 }
 int mgp_relax_residual(mgp_solver* s, int l, double omega, int64_t nsmooth, double* norm) {
     CKS(validate_level(s, l));

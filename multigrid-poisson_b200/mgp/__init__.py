@@ -118,6 +118,7 @@ def lib():
         L.mgp_solve.argtypes = [vp, i32, i64, dbl, ctypes.c_char_p, dbl, ctypes.c_uint32, ctypes.POINTER(Stats)]
         L.mgp_set_iteration_limits.argtypes = [vp, i64, i64, dbl]
         L.mgp_relax.argtypes = [vp, i32, dbl, i64]
+        L.mgp_relax_colour.argtypes = [vp, i32, dbl, i32]
         L.mgp_set_wait_polls.argtypes = [vp, i64]
         L.mgp_set_tuning.argtypes = [vp, i32, i32, i64]
         L.mgp_get_tuning.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
@@ -337,6 +338,10 @@ class Solver:
     # ---- operators ----
     def relax(self, level, omega=-1.0, nsmooth=1):
         _check(lib().mgp_relax(self._h, level, omega, nsmooth))
+
+    def relax_colour(self, level, omega=-1.0, colour=0):
+        """One red-black half-sweep of one colour (mgp_relax_colour); alternate flag untouched."""
+        _check(lib().mgp_relax_colour(self._h, level, omega, colour))
 
     def set_wait_polls(self, polls):
         """Bound of the wavefront passes' waits for a plane copy (0: the default)."""

@@ -19,9 +19,15 @@ solve, point for point:
   fine plane 2I-1, and the prolongation reads coarse plane I+1.
 * Norms run over owned planes only and combine as a max (an all-reduce MAX between processes).
 
-Weighted Jacobi only: a red-black half-sweep would need its own exchange between the two
-colours, and a slab keeps the reference's colouring (the parity of the padded linear index)
-only when its offset times the plane stride is even.
+Relaxation: weighted Jacobi (one sweep at a time, exchanged in between), or red-black
+Gauss-Seidel as ordered half-sweeps of one colour each, exchanged in between (a point of one
+colour reads only the other colour).  The colour of a point is the parity of the reference's
+padded linear index in the ONE-domain layout (include/gaussseidel.h:56,81).  A slab's own
+layout has the same padded y/z extents P_y, P_z but its own west halo w_s (0 at a cut, which is
+Dirichlet) and starts at global plane lo, so its padded index differs from the global one by
+(lo + w_g - w_s) * P_y * P_z: where that is odd, the slab sweeps the other local colour.  With
+P_y * P_z even the colour does not depend on i at all (x-neighbours share a colour and the
+one-domain sweep runs column by column in i order); such layouts are refused.
 
 Exchange: ranks in one process copy planes directly; ranks in different processes send them
 with torch.distributed point-to-point operations (NCCL between GPUs, gloo on the host).  Each
@@ -177,14 +183,38 @@ class DistExchange:
 # ---- the decomposed solve -------------------------------------------------------------------
 class SlabSolver:
     """The reference's solve loop and V/F-cycles (include/libpoisson.h:237-357,
-    include/vcycle.h:14-98, include/fcycle.h:13-97) with Jacobi smoothing over slabs, one
-    operation at a time with the halo exchanges between them.  Executors provide the level
-    operations of one slab (relax, residual, restrict, restrict_bc, zero_u, prolong_add, the
-    max-norm over owned planes) and plane access."""
+    include/vcycle.h:14-98, include/fcycle.h:13-97) over slabs, one operation at a time with the
+    halo exchanges between them.  Executors provide the level operations of one slab (relax,
+    relax_colour, residual, restrict, restrict_bc, zero_u, prolong_add, the max-norm over owned
+    planes), plane access and, for red-black smoothing, layout(level) = (west halo, P_y * P_z)
+    of their own padded layout.
 
-    def __init__(self, slabs: list, comm, levels: int, omega: float, maxiter: int, miniter: int = 1, tol: float = 0.0):
+    relaxation: "jacobi" or "gs"; west_halo: the west halo width of the one-domain layout
+    (global_west_halo), which fixes the red-black colours."""
+
+    def __init__(self, slabs: list, comm, levels: int, omega: float, maxiter: int, miniter: int = 1, tol: float = 0.0,
+                 relaxation: str = "jacobi", west_halo: int | None = None):
         self.slabs, self.comm, self.levels = slabs, comm, levels
         self.omega, self.maxiter, self.miniter, self.tol = omega, maxiter, miniter, tol
+        self.gs = relaxation.lower() in ("gs", "gaussseidel", "gauss-seidel")
+        if self.gs and west_halo is None:
+            raise ValueError("red-black smoothing needs the one-domain west halo width (global_west_halo)")
+        self.west_halo = west_halo
+        self.alternate = True  # GaussSeidel::alternate (include/gaussseidel.h:18): colour 0 first
+        if self.gs:
+            # with P_y * P_z even the colour does not depend on i: x-neighbours share a colour, the
+            # one-domain half-sweep runs in i order (column-ordered) and does not split into slabs
+            for r in comm.ranks():
+                for l in range(levels):
+                    if comm.ex[r].layout(l)[1] % 2 == 0:
+                        raise ValueError("red-black layout with an even padded y*z extent: the colours do not "
+                                         "alternate along x, so the sweep cannot be split into x-slabs")
+
+    def colour_flip(self, rank: int, l: int) -> int:
+        """1 where the slab's padded index parity differs from the one-domain layout's."""
+        lo = self.slabs[rank].at(l)[0]
+        w_s, pyz = self.comm.ex[rank].layout(l)
+        return ((lo + self.west_halo - w_s) * pyz) & 1
 
     # level operations on every local slab, each followed by the exchange it needs
     def _each(self, fn):
@@ -192,9 +222,17 @@ class SlabSolver:
             fn(self.comm.ex[r])
 
     def relax(self, l: int, ns: int) -> None:
-        for _ in range(ns):  # Jacobi: one sweep at a time, exchanged in between
-            self._each(lambda e: e.relax(l, self.omega, 1))
+        if not self.gs:
+            for _ in range(ns):  # Jacobi: one sweep at a time, exchanged in between
+                self._each(lambda e: e.relax(l, self.omega, 1))
+                self.comm.exchange(self.slabs, "u", l)
+            return
+        for _ in range(2 * ns):  # red-black: one colour at a time (relaxation.h:19-94)
+            colour = 0 if self.alternate else 1
+            for r in self.comm.ranks():
+                self.comm.ex[r].relax_colour(l, self.omega, colour ^ self.colour_flip(r, l))
             self.comm.exchange(self.slabs, "u", l)
+            self.alternate = not self.alternate
 
     def setup(self, l: int) -> None:
         self._each(lambda e: e.residual(l))
@@ -259,19 +297,40 @@ class SlabSolver:
         return rel, it, hist
 
 
+def global_west_halo(mgp, dims, levels, h, bc_requested, restriction, relaxation, strict_bc=False) -> int:
+    """West halo width of the one-domain layout (the reference's Domain halo for the resolved
+    west face kind), planned from the descriptor alone (mgp_plan_level, no device needed)."""
+    import ctypes
+
+    d = mgp.make_desc(dims, levels, h, bc_requested, restriction, relaxation, mgp.F64, 1, 1, 0.0, (0.0, 0.0, 0.0), 0,
+                      strict_bc, 0)
+    li = mgp.LevelInfo()
+    mgp._check(mgp.lib().mgp_plan_level(ctypes.byref(d), 0, ctypes.byref(li)))
+    return int(li.halo[1])  # halo order: east, west, north, south, top, bottom
+
+
 # ---- the engine executor (one CUDA solver per slab) ----------------------------------------
 class EngineSlab:
     """One slab on one GPU: a plain engine solver over the slab's planes (the global requested
     boundary kinds and strict flag, Dirichlet at the cuts), driven one level operation at a
     time."""
 
-    def __init__(self, mgp, slab: Slab, dims, levels, h, bc_requested, restriction, strict_bc=False, device=0):
+    def __init__(self, mgp, slab: Slab, dims, levels, h, bc_requested, restriction, strict_bc=False, device=0,
+                 relaxation=None):
         import torch
 
         self.mgp, self.slab, self.torch = mgp, slab, torch
+        rlx = mgp.JACOBI if relaxation is None else relaxation
         self.solver = mgp.Solver((slab.nx, dims[1], dims[2]), levels, h, slab_bc(slab, bc_requested), restriction,
-                                 mgp.JACOBI, mgp.F64, 1, 1, 0.0, device=device, strict_bc=strict_bc)
+                                 rlx, mgp.F64, 1, 1, 0.0, device=device, strict_bc=strict_bc)
         self.comm_device = torch.device("cuda", device)
+
+    def layout(self, l):
+        lv = self.solver.level[l]
+        return lv.halo["west"], lv.pad[1] * lv.pad[2]
+
+    def relax_colour(self, l, omega, colour):
+        self.solver.relax_colour(l, omega, colour)
 
     def _planes(self, field: str, level: int):
         """The field's buffer as (nx, plane pitch) -- looked up each time: Jacobi sweeps swap

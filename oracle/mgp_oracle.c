@@ -384,6 +384,17 @@ void orc_relax(orc_solver* S, int l, double omega, long nsmooth) {
     }
 }
 
+/* One red-black half-sweep of the given colour (the parity of the padded linear index), ghosts
+ * refreshed first as orc_relax does; the alternate flag is left as it was.  The decomposed
+ * solve orders the colours itself and exchanges halo planes between them. */
+void orc_relax_colour(orc_solver* S, int l, double omega, int colour) {
+    const int keep = S->gs_alternate;
+    S->gs_alternate = colour == 0;
+    update_ghosts(S, l, S->u[l]);
+    gs_kernel(S, l, omega);
+    S->gs_alternate = keep;
+}
+
 /* residual<T> (include/residual.h:17-81). */
 void orc_residual(orc_solver* S, int l) {
     orc_level* L = &S->lv[l];

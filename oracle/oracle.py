@@ -88,6 +88,7 @@ def lib():
                      "orc_prolong", "orc_add"):
             getattr(L, name).argtypes = [vp, ctypes.c_int]
         L.orc_relax.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_long]
+        L.orc_relax_colour.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.orc_vcycle.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_long]
         L.orc_fcycle.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_long]
         L.orc_norm.argtypes = [vp, ctypes.c_int, ctypes.c_int]
@@ -178,6 +179,10 @@ class Oracle:
 
     def relax(self, level, omega, nsmooth):
         lib().orc_relax(self._h, level, omega, nsmooth)
+
+    def relax_colour(self, level, omega, colour):
+        """One red-black half-sweep of one colour; the alternate flag is left as it was."""
+        lib().orc_relax_colour(self._h, level, omega, colour)
 
     def residual(self, level):
         lib().orc_residual(self._h, level)

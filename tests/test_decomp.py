@@ -1,7 +1,9 @@
 """CPU: domain decomposition along x (mgp/decomp.py).  The planner's slabs nest over the levels
 and cover every plane once; the decomposed solve -- each slab an oracle hierarchy over its
-planes, halo planes exchanged after every operation -- reproduces the one-domain oracle solve
-bit for bit at every owned plane, with the slabs in one process and as two gloo ranks."""
+planes, halo planes exchanged after every operation (after every half-sweep with red-black
+smoothing, each slab sweeping the colour that is the one-domain colour in its own layout) --
+reproduces the one-domain oracle solve bit for bit at every owned plane, with Jacobi and with
+red-black Gauss-Seidel, the slabs in one process and as two gloo ranks."""
 import os
 import tempfile
 
@@ -15,6 +17,7 @@ from mgp import decomp
 from oracle.oracle import Oracle
 
 RST = {"inj": 0, "fw": 1}
+RLX = {"jacobi": 0, "gs": 1}
 
 
 class OracleSlab:
@@ -23,14 +26,14 @@ class OracleSlab:
 
     comm_device = torch.device("cpu")
 
-    def __init__(self, slab, g: Oracle, bc, levels, h, rst):
+    def __init__(self, slab, g: Oracle, bc, levels, h, rst, rlx="jacobi"):
         self.slab = slab
         nx, ny, nz = g.meta[0].shape
-        self.o = Oracle((slab.nx, ny, nz), levels, h, decomp.slab_bc(slab, bc), RST[rst], 0, False)
+        self.o = Oracle((slab.nx, ny, nz), levels, h, decomp.slab_bc(slab, bc), RST[rst], RLX[rlx], False)
         m, gm = self.o.meta[0], g.meta[0]
         self.hw = m.halo["west"]
         off = slab.lo + gm.halo["west"] - self.hw  # global padded x index of local padded 0
-        for name in ("u", "uprev", "f", "r"):
+        for name in fields_of(rlx):
             self.o.field(name, 0)[...] = g.field(name, 0)[off:off + m.pad[0]]
         for fc in range(6):
             gf, lf = g.face(fc, 0), self.o.face(fc, 0)
@@ -55,6 +58,13 @@ class OracleSlab:
 
     def relax(self, l, omega, ns):
         self.o.relax(l, omega, ns)
+
+    def relax_colour(self, l, omega, colour):
+        self.o.relax_colour(l, omega, colour)
+
+    def layout(self, l):
+        m = self.o.meta[l]
+        return m.halo["west"], m.pad[1] * m.pad[2]
 
     def residual(self, l):
         self.o.residual(l)
@@ -83,19 +93,30 @@ class OracleSlab:
 
 
 CASES = [
-    # dims, levels, requested bc (N S E W T B), restriction, cycle, nsmooth, parts
-    ((65, 17, 17), 3, (1, 1, 1, 1, 0, 0), "fw", "Vcycle", 2, 2),
-    ((97, 17, 9), 3, (0, 0, 1, 0, 1, 0), "inj", "Fcycle", 3, 3),
-    ((129, 9, 17), 4, (1, 0, 0, 1, 0, 1), "fw", "Fcycle", 2, 4),
-    ((33, 9, 9), 1, (0, 0, 0, 1, 0, 0), "fw", "Vcycle", 4, 3),  # one level: relaxation only, H = 1
+    # dims, levels, requested bc (N S E W T B), restriction, cycle, nsmooth, parts, relaxation
+    ((65, 17, 17), 3, (1, 1, 1, 1, 0, 0), "fw", "Vcycle", 2, 2, "jacobi"),
+    ((97, 17, 9), 3, (0, 0, 1, 0, 1, 0), "inj", "Fcycle", 3, 3, "jacobi"),
+    ((129, 9, 17), 4, (1, 0, 0, 1, 0, 1), "fw", "Fcycle", 2, 4, "jacobi"),
+    ((33, 9, 9), 1, (0, 0, 0, 1, 0, 0), "fw", "Vcycle", 4, 3, "jacobi"),  # one level: relaxation only, H = 1
+    # red-black: padded y*z extent odd (N/S alike, T/B alike, odd ny, nz), so slabs whose offset
+    # (+ the global west halo) is odd sweep the other local colour
+    ((65, 17, 17), 3, (1, 1, 1, 1, 0, 0), "fw", "Vcycle", 2, 2, "gs"),  # Neumann west: every cut slab flips
+    ((97, 17, 9), 3, (0, 0, 1, 0, 1, 1), "inj", "Fcycle", 3, 3, "gs"),  # flips on the coarsest level only
+    ((129, 17, 17), 4, (1, 1, 0, 1, 0, 0), "fw", "Fcycle", 2, 4, "gs"),
+    ((129, 17, 17), 4, (0, 0, 0, 0, 0, 0), "inj", "Vcycle", 3, 3, "gs"),  # all Dirichlet
 ]
+FLIPPING = (4, 5, 6)  # red-black cases where some slab sweeps the other local colour
 
 
-def global_state(dims, levels, bc, rst, seed):
+def fields_of(rlx):
+    return ("u", "uprev", "f", "r") if rlx == "jacobi" else ("u", "f", "r")
+
+
+def global_state(dims, levels, bc, rst, seed, rlx="jacobi"):
     h = 1.0 / (dims[0] - 1)
-    g = Oracle(dims, levels, h, bc, RST[rst], 0, False)
+    g = Oracle(dims, levels, h, bc, RST[rst], RLX[rlx], False)
     rng = np.random.default_rng(seed)
-    for name in ("u", "uprev", "f", "r"):
+    for name in fields_of(rlx):
         g.field(name, 0)[...] = rng.uniform(-1, 1, size=g.meta[0].pad)
     for fc in range(6):
         g.face(fc, 0)[...] = rng.uniform(-1, 1, size=g.face(fc, 0).shape)
@@ -128,22 +149,23 @@ def test_plan_slabs_nest_and_cover():
         decomp.plan_slabs(17, 3, 5)
 
 
-def run_slabs_local(dims, levels, bc, rst, cycle, ns, parts, seed):
-    g, h = global_state(dims, levels, bc, rst, seed)
+def run_slabs_local(dims, levels, bc, rst, cycle, ns, parts, rlx, seed):
+    g, h = global_state(dims, levels, bc, rst, seed, rlx)
     slabs = decomp.plan_slabs(dims[0], levels, parts)
-    ex = {s.rank: OracleSlab(s, g, bc, levels, h, rst) for s in slabs}
+    ex = {s.rank: OracleSlab(s, g, bc, levels, h, rst, rlx) for s in slabs}
     omega = g.default_omega()
-    solver = decomp.SlabSolver(slabs, decomp.LocalExchange(ex), levels, omega, maxiter=3)
+    solver = decomp.SlabSolver(slabs, decomp.LocalExchange(ex), levels, omega, maxiter=3, relaxation=rlx,
+                               west_halo=g.meta[0].halo["west"])
     rel, it, hist = solver.solve(cycle, ns)
     rr, it_g, _, hist_g = g.solve(cycle, ns, omega, 3, 1, 0.0)
-    return g, slabs, ex, (rel, it, hist), (rr, it_g, hist_g)
+    return g, slabs, ex, solver, (rel, it, hist), (rr, it_g, hist_g)
 
 
 @pytest.mark.parametrize("ci", range(len(CASES)))
 def test_slabs_in_one_process_match_global_solve(ci):
-    dims, levels, bc, rst, cycle, ns, parts = CASES[ci]
-    g, slabs, ex, (rel, it, hist), (rr, it_g, hist_g) = run_slabs_local(dims, levels, bc, rst, cycle, ns, parts,
-                                                                        100 + ci)
+    dims, levels, bc, rst, cycle, ns, parts, rlx = CASES[ci]
+    g, slabs, ex, solver, (rel, it, hist), (rr, it_g, hist_g) = run_slabs_local(dims, levels, bc, rst, cycle, ns,
+                                                                                parts, rlx, 100 + ci)
     assert rel == rr and it == it_g
     assert hist[1:] == list(hist_g)  # the oracle's history starts after the initial residual
     for name in ("u", "r"):
@@ -151,17 +173,46 @@ def test_slabs_in_one_process_match_global_solve(ci):
         for s in slabs:
             _, _, olo, ohi = s.at(0)
             assert np.array_equal(ex[s.rank].owned(name), whole[olo:ohi]), (name, s.rank)
+    if ci in FLIPPING:
+        assert any(solver.colour_flip(s.rank, l) for s in slabs for l in range(levels))
+
+
+def test_red_black_layout_without_x_alternation_is_refused():
+    """P_y even (one Neumann, one Dirichlet face in y): the colour does not depend on i."""
+    dims, levels, bc, rst = (65, 17, 17), 3, (1, 0, 1, 1, 0, 0), "fw"
+    g, h = global_state(dims, levels, bc, rst, 7, "gs")
+    slabs = decomp.plan_slabs(dims[0], levels, 2)
+    ex = {s.rank: OracleSlab(s, g, bc, levels, h, rst, "gs") for s in slabs}
+    with pytest.raises(ValueError):
+        decomp.SlabSolver(slabs, decomp.LocalExchange(ex), levels, 1.0, maxiter=1, relaxation="gs",
+                          west_halo=g.meta[0].halo["west"])
+
+
+def test_global_west_halo_matches_the_one_domain_layout():
+    import mgp
+
+    for dims, levels, bc, rst, _, _, _, rlx in CASES:
+        g, h = global_state(dims, levels, bc, rst, 0, rlx)
+        got = decomp.global_west_halo(mgp, dims, levels, h, bc, RST[rst], RLX[rlx])
+        assert got == g.meta[0].halo["west"], (dims, bc)
+
+
+def test_red_black_needs_the_global_west_halo():
+    slabs = decomp.plan_slabs(65, 3, 2)
+    with pytest.raises(ValueError):
+        decomp.SlabSolver(slabs, None, 3, 1.0, maxiter=1, relaxation="gs")
 
 
 def _gloo_rank(rank, world, port, case, seed, out_dir):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        dims, levels, bc, rst, cycle, ns, parts = case
-        g, h = global_state(dims, levels, bc, rst, seed)
+        dims, levels, bc, rst, cycle, ns, parts, rlx = case
+        g, h = global_state(dims, levels, bc, rst, seed, rlx)
         slabs = decomp.plan_slabs(dims[0], levels, world)
-        e = OracleSlab(slabs[rank], g, bc, levels, h, rst)
-        solver = decomp.SlabSolver(slabs, decomp.DistExchange(e, rank, world), levels, g.default_omega(), maxiter=3)
+        e = OracleSlab(slabs[rank], g, bc, levels, h, rst, rlx)
+        solver = decomp.SlabSolver(slabs, decomp.DistExchange(e, rank, world), levels, g.default_omega(), maxiter=3,
+                                   relaxation=rlx, west_halo=g.meta[0].halo["west"])
         rel, it, hist = solver.solve(cycle, ns)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), u=e.owned("u"), r=e.owned("r"), rel=rel, it=it,
                  hist=np.array(hist))
@@ -169,15 +220,15 @@ def _gloo_rank(rank, world, port, case, seed, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("ci", [0, 2])
+@pytest.mark.parametrize("ci", [0, 2, 4, 6])
 def test_slabs_as_two_gloo_ranks_match_global_solve(ci):
-    case = CASES[ci][:6] + (2,)
-    dims, levels, bc, rst, cycle, ns, _ = case
+    case = CASES[ci][:6] + (2, CASES[ci][7])
+    dims, levels, bc, rst, cycle, ns, _, rlx = case
     port = 29500 + (os.getpid() % 1000) + ci
     with tempfile.TemporaryDirectory() as d:
         mp.start_processes(_gloo_rank, args=(2, port, case, 300 + ci, d), nprocs=2, join=True, start_method="spawn")
         res = [np.load(os.path.join(d, f"rank{r}.npz")) for r in range(2)]
-        g, h = global_state(dims, levels, bc, rst, 300 + ci)
+        g, h = global_state(dims, levels, bc, rst, 300 + ci, rlx)
         rr, it_g, _, hist_g = g.solve(cycle, ns, g.default_omega(), 3, 1, 0.0)
         slabs = decomp.plan_slabs(dims[0], levels, 2)
         for r, s in enumerate(slabs):
