@@ -602,9 +602,10 @@ def cpu_reference(steps: int, warm: int, threads: int | None = None):
 
 
 def cpu_reference_best(cycles: int, warm: int):
-    """The reference's CPU build at its fastest OpenMP thread count: one timed cycle at each of
-    1, 2, 4, ..., nproc threads (its build can be slower with more threads), then the bounded
-    sample of `cycles` cycles after `warm` warm-up cycles at the fastest count."""
+    """The reference's CPU build at its fastest OpenMP thread count: one timed cycle after one
+    warm-up cycle at each of 1, 2, 4, ..., nproc threads (its build can be slower with more
+    threads; the first cycle after allocation also pays the arrays' first-touch page faults),
+    then the bounded sample of `cycles` cycles after `warm` warm-up cycles at the fastest count."""
     nproc = os.cpu_count() or 1
     counts = []
     t = 1
@@ -614,7 +615,7 @@ def cpu_reference_best(cycles: int, warm: int):
     counts.append(nproc)
     sweep = {}
     for t in counts:
-        r = cpu_reference(1, 0, threads=t)
+        r = cpu_reference(1, 1, threads=t)
         if r is None:
             return None
         sweep[t] = r["value"]
@@ -777,7 +778,7 @@ def main():
     cpu = None
     if not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference_best(CPU_BASELINE_CYCLES, 0)
+            cpu = cpu_reference_best(CPU_BASELINE_CYCLES, 1)
         except Exception as exc:  # noqa: BLE001 -- the baseline is informative only
             cpu = {"error": str(exc)}
     clocks = clk.summary()
@@ -817,8 +818,9 @@ def main():
                 line[key] = {"error": repr(exc)}
     if cpu and "value" in cpu:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["threads"], "kind": "reference",
-                                "sample": f"{int(cpu['cycles'])} F-cycles of the same workload, reference OpenMP "
-                                          f"build, OMP_NUM_THREADS={cpu['threads']} (fastest of a thread sweep)",
+                                "sample": f"{int(cpu['cycles'])} F-cycles of the same workload after "
+                                          f"{cpu['warm']} warm-up cycle, reference OpenMP build, "
+                                          f"OMP_NUM_THREADS={cpu['threads']} (fastest of a thread sweep)",
                                 "thread_sweep": cpu.get("sweep")}
     elif cpu:
         line["cpu_baseline"] = {"error": cpu.get("error")}
