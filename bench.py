@@ -47,10 +47,11 @@ NSMOOTH = 2
 E2E_CYCLES = 4
 REF_ARM_CYCLES = 30   # timed cycles of the reference arm (a bounded sample)
 # DRAM bytes (read + write) of one level-0 Jacobi sweep launch at this size, from an ncu capture
-# of two launches: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-#   --clock-control none -k regex:k_stencil -c 2 python bench.py --kernels --steps 1
-# (408.6 MB and 404.0 MB; algorithmic 408.2 MB).
-JACOBI_SWEEP_DRAM_BYTES = 406.3e6
+# of the timed launch: ncu --set full --clock-control none --kernel-name-base demangled
+#   -k "regex:k_stencil<double, \(int\)0, \(bool\)0, \(bool\)0>" -s 3 -c 1 python bench.py --kernels --steps 1
+# (289.6 MB read + 109.7 MB written; algorithmic 408.2 MB: some of u is still in L2 from the
+# launch before).
+JACOBI_SWEEP_DRAM_BYTES = 399.3e6
 CPU_BASELINE_CYCLES = 8
 NDOF = DIMS[0] * DIMS[1] * DIMS[2]
 METRIC = "F-cycle fine-grid DOF/s (FP64, 513x257x129)"
@@ -792,7 +793,7 @@ def main():
                 "step": f"to_device + {E2E_CYCLES}-cycle solve + to_host", "ms_per_request": 1e3 * e2e_sec},
         "roofline": {"bound": "hbm", "kernel": "k_stencil<double,OP_JACOBI> level 0", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": JACOBI_SWEEP_DRAM_BYTES, "traffic_source": "ncu dram__bytes_read+write, 2 launches",
+                     "traffic": JACOBI_SWEEP_DRAM_BYTES, "traffic_source": "ncu dram__bytes_read+write, 1 launch",
                      "algorithmic_bytes_per_launch": kbytes, "launch_us": ksec * 1e6},
         "cycle_roofline": {"model_bytes_per_cycle": cyc_bytes, "achieved": cyc_achieved, "peak": peak,
                            "unit": "GB/s", "frac": cyc_achieved / peak, "ms_per_cycle": 1e3 * sec / args.steps},
