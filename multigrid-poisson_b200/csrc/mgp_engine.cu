@@ -138,6 +138,10 @@ struct mgp_solver {
     // inner solver shares this solver's stream.
     mgp_solver* inner = nullptr;
     bool owns_stream = true;
+    // Side stream of the coarse-grid set-up: the Neumann face restriction runs on it, forked
+    // and joined by the two events, overlapped with the residual (own-memory solvers only).
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // Problems of a batch allocate from the batch's memory pool in the batch's stream order
     // (no device-wide synchronisation when they come and go) and read norms back through the
     // batch's pinned slab.
@@ -798,7 +802,7 @@ template <typename T>
 BcRestrictArgs<T> bc_args(mgp_solver* s, int l, bool* any);
 
 template <typename T>
-int restrict_bc_t(mgp_solver* s, int l) {
+int restrict_bc_t(mgp_solver* s, int l, cudaStream_t on = nullptr) {
     bool any = false;
     BcRestrictArgs<T> a = bc_args<T>(s, l, &any);
     // Dirichlet faces: coarse g = 0 (dirichlet.h:101-107).  Coarse Dirichlet arrays are
@@ -809,6 +813,15 @@ int restrict_bc_t(mgp_solver* s, int l) {
     for (int f = 0; f < 6; f++)
         nmax = std::max(nmax, (long long)(C.face_shape[f][0] * C.face_shape[f][1] * C.face_shape[f][2]));
     dim3 grid((unsigned)std::max(1ll, std::min((nmax + kThreads - 1) / kThreads, 4096ll)), 6);
+    if (on) {  // the side stream: an ordinary launch after the fork event
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(kThreads);
+        cfg.stream = on;
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, k_restrict_bc<T>, a);
+        if (e != cudaSuccess) return fail(MGP_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+        return check_launch(s);
+    }
     return launch_k(s, k_restrict_bc<T>, grid, dim3(kThreads), 0, a);
 }
 
@@ -1017,8 +1030,20 @@ int coarse_setup_t(mgp_solver* s, int l, double omega, int64_t ns, bool resid_do
     if (!setup_residual_separate(s, l)) {
         CKS(coarse_setup_fused_t<T>(s, l, w));
     } else {
-        if (!resid_done) CKS(residual_t<T>(s, l, nullptr));
-        CKS(restrict_bc_t<T>(s, l));  // before the restriction: the first sweep reads the coarse faces
+        // The face restriction (reads u and the fine faces) and the residual (reads u, writes r)
+        // are independent: the face restriction runs on the side stream meanwhile, joined before
+        // the restriction, whose first coarse sweep reads the coarse faces.
+        if (!resid_done && s->side) {
+            CK(cudaEventRecord(s->ev_fork, s->stream));
+            CK(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+            CKS(restrict_bc_t<T>(s, l, s->side));
+            CK(cudaEventRecord(s->ev_join, s->side));
+            CKS(residual_t<T>(s, l, nullptr));
+            CK(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+        } else {
+            if (!resid_done) CKS(residual_t<T>(s, l, nullptr));
+            CKS(restrict_bc_t<T>(s, l));
+        }
         CKS(restrict_t<T>(s, l, /*zero_coarse_u=*/true, w));
     }
     s->lv[l + 1].first_done = w.on != 0;
@@ -1487,6 +1512,9 @@ void release(mgp_solver* s) {
     dev_free(s, s->stage);
     if (s->inner) release(s->inner);
     if (s->stream && s->owns_stream) cudaStreamDestroy(s->stream);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
     delete s;
 }
 
@@ -1636,6 +1664,12 @@ static int create_plain(const mgp_desc* d, mgp_solver** out, const CreateCtx* ct
         s->stream = nullptr;
         release(s);
         return fail(MGP_ERR_CUDA, "stream creation failed");
+    }
+    if (!s->pool && (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
+        release(s);
+        return fail(MGP_ERR_CUDA, "side stream creation failed");
     }
     s->lv.resize(s->levels);
     for (int l = 0; l < s->levels; l++) {
