@@ -237,3 +237,62 @@ def test_slabs_as_two_gloo_ranks_match_global_solve(ci):
             _, _, olo, ohi = s.at(0)
             for name in ("u", "r"):
                 assert np.array_equal(res[r][name], g.shape_view(name, 0)[olo:ohi]), (name, r)
+
+
+class _LayoutOnly:
+    """Executor stand-in that only reports a slab's layout (its own oracle metadata)."""
+
+    def __init__(self, o):
+        self.o = o
+
+    def layout(self, l):
+        m = self.o.meta[l]
+        return m.halo["west"], m.pad[1] * m.pad[2]
+
+
+def test_colour_flip_is_the_padded_index_parity_difference():
+    """For random geometries, every slab and level: the colour a slab sweeps differs from the
+    one-domain colour exactly where the padded linear indices of the same point differ in
+    parity (the reference's colour rule, include/gaussseidel.h:56,81)."""
+    rng = np.random.default_rng(5)
+    checked = 0
+    for _ in range(40):
+        levels = int(rng.integers(1, 5))
+        H = 1 << (levels - 1)
+        nx = H * int(rng.integers(4, 12)) + 1
+        ny = (1 << (levels - 1)) * int(rng.integers(1, 4)) + 1
+        nz = (1 << (levels - 1)) * int(rng.integers(1, 4)) + 1
+        bc = tuple(int(x) for x in rng.integers(0, 2, size=6))
+        parts = int(rng.integers(2, 5))
+        try:
+            slabs = decomp.plan_slabs(nx, levels, parts)
+        except ValueError:
+            continue
+        h = 1.0 / (nx - 1)
+        g = Oracle((nx, ny, nz), levels, h, bc, 1, 1, False)
+        ex = {s.rank: _LayoutOnly(Oracle((s.nx, ny, nz), levels, h, decomp.slab_bc(s, bc), 1, 1, False))
+              for s in slabs}
+
+        class _Comm:
+            def __init__(self, ex):
+                self.ex = ex
+
+            def ranks(self):
+                return sorted(self.ex)
+
+        solver = decomp.SlabSolver.__new__(decomp.SlabSolver)
+        solver.slabs, solver.comm, solver.west_halo = slabs, _Comm(ex), g.meta[0].halo["west"]
+        for s in slabs:
+            for l in range(levels):
+                gm, lm = g.meta[l], ex[s.rank].o.meta[l]
+                lo = s.at(l)[0]
+                for il in (0, 1, s.at(l)[1] - lo):  # a few planes of the slab
+                    for j, k in ((0, 0), (1, 0), (0, 1), (gm.shape[1] - 1, gm.shape[2] - 1)):
+                        def idx(m, i):
+                            return (((i + m.halo["west"]) * m.pad[1] + j + m.halo["south"]) * m.pad[2] + k
+                                    + m.halo["bottom"])
+
+                        diff = (idx(gm, il + lo) - idx(lm, il)) & 1
+                        assert diff == solver.colour_flip(s.rank, l), (nx, ny, nz, bc, levels, parts, s.rank, l)
+                        checked += 1
+    assert checked > 100
